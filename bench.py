@@ -1,0 +1,369 @@
+#!/usr/bin/env python3
+"""Benchmark: the 30-qubit depth-40 random circuit (brickwork RX/RY/RZ +
+CNOT, a ZZ layer every 4 layers) on the B200 engine.
+
+One step = prepare |0...0> and run the whole 4470-gate circuit (4180 one-
+and two-qubit gates + 290 ZZ) on a complex128 state (16 GiB), the plain
+drop-in path; the same circuit on a complex64 state (8 GiB) is reported
+beside it.  `value` is circuits/s over all ranks, device-timed with CUDA
+events on the engine's stream; `e2e` is the same metric through the public
+C ABI from host gate records to host results (<Z_i> for every qubit and
+1024 sampled outcomes read back) each step.
+
+`--impl reference` times the reference's own CPU implementation
+(oracle/_ref/liboracle.so, built from its sources; all host threads) on a
+bounded, stratified sample of the same circuit and extrapolates per gate.
+
+Multi-GPU: one process per GPU (torchrun); each rank runs its own circuit
+replica (the workload does not shard below 34 qubits), timing is the max
+over ranks, and value = circuits of all ranks / that time ("weak").
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "30q circuit time & HBM GB/s (fused c64 vs plain c128); circuits/s, p99 at load"
+WORKLOAD = "30q depth-40 brickwork RX/RY/RZ+CNOT, ZZ(theta) layer every 4 layers (4470 gates)"
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path: stratified per-gate sample of the circuit
+# ---------------------------------------------------------------------------
+def reference_sample(n: int, budget_s: float, gates):
+    """Time the reference library's gate_* calls at n qubits on a stratified
+    sample (each gate type at low / middle / high targets) and extrapolate
+    the full circuit.  Returns (circuit_seconds, sample_description, cores,
+    kind)."""
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    from oracle import bindings as B
+    if B.have_ref():
+        r = B.RefStateVector(n)
+        kind = "reference"
+    else:
+        raise RuntimeError("reference library oracle/_ref/liboracle.so not built")
+    L, p = r.lib, C.byref(r.s)
+    targets = [0, 1, n // 2, n - 2]
+    kinds = {
+        "rx": lambda q: L.gate_rx(p, q, 0.3), "ry": lambda q: L.gate_ry(p, q, 0.4),
+        "rz": lambda q: L.gate_rz(p, q, 0.5), "cnot": lambda q: L.gate_cnot(p, q, q + 1),
+    }
+    per = {}
+    t_start = time.perf_counter()
+    reps = 0
+    while True:
+        for k, f in kinds.items():
+            for q in targets:
+                t0 = time.perf_counter()
+                f(q)
+                per.setdefault(k, []).append(time.perf_counter() - t0)
+        reps += 1
+        if time.perf_counter() - t_start > budget_s or reps >= 4:
+            break
+    mean = {k: sum(v) / len(v) for k, v in per.items()}
+    counts = {k: int(np.sum(gates["type"] == t)) for k, t in (("rx", 7), ("ry", 8), ("rz", 9), ("cnot", 10))}
+    nzz = int(np.sum(gates["type"] == 27))
+    total = sum(mean[k] * counts[k] for k in counts) + nzz * (2 * mean["cnot"] + mean["rz"])
+    sample = (f"{reps * len(targets) * len(kinds)} gate_* calls at {n} qubits (RX/RY/RZ/CNOT at "
+              f"targets {targets}), {time.perf_counter() - t_start:.1f} s; circuit time extrapolated "
+              f"per gate over {len(gates)} gates (ZZ = CNOT.RZ.CNOT)")
+    r.close()
+    return total, sample, int(os.environ.get("OMP_NUM_THREADS", cores)), kind
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def dist_done(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, ws, rank):
+    from moonlab_b200.circuits import config_c2
+    if rank != 0:
+        return
+    gates, _ = config_c2(args.qubits, args.depth)
+    step_vals = []
+    samples = []
+    for i in range(args.warmup + args.steps):
+        secs, sample, cores, kind = reference_sample(args.qubits, args.ref_budget, gates)
+        if i >= args.warmup:
+            step_vals.append(secs)
+            samples.append(sample)
+    secs = statistics.median(step_vals)
+    val = 1.0 / secs
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "circuits/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic seeded circuit (splitmix64 0xC2)",
+            "config": {"workload": WORKLOAD, "qubits": args.qubits, "depth": args.depth},
+            "cpu_baseline": {"value": val, "unit": "circuits/s", "cores": cores, "kind": kind,
+                             "sample": samples[-1]},
+            "e2e": {"value": val, "unit": "circuits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, ws, rank, local):
+    import torch
+    from moonlab_b200 import StateVector, _lib, kernel_launches
+    from moonlab_b200.circuits import config_c2
+
+    torch.cuda.set_device(local)
+    gates, shots = config_c2(args.qubits, args.depth)
+    n = args.qubits
+    sv = StateVector(n, "c128", device=local)
+    sv.set_timing(True)
+    stream = torch.cuda.ExternalStream(sv.stream(), device=torch.device("cuda", local))
+
+    def step():
+        sv.reset()
+        sv.run(gates)
+        sv.flush()
+
+    # warm-up
+    for _ in range(args.warmup):
+        step()
+        sv.synchronize()
+    dist_barrier(ws)
+    torch.cuda.synchronize()
+    launches0 = kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pass_ms = []
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+            st = sv.flush_stats()  # waits for this step's kernels (device events)
+            pass_ms.append(st["gpu_ms"] / max(1, st["passes"]))
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    dist_barrier(ws)
+    launches = kernel_launches() - launches0
+    t = ev0.elapsed_time(ev1) / 1e3 / args.steps
+    t_max = dist_max(t, ws)
+    st = sv.flush_stats()
+    passes = int(st["passes"])
+    per_pass_bytes = 2 * 16 * (1 << n)
+    avg_pass_s = statistics.median(pass_ms) / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = per_pass_bytes / avg_pass_s / 1e9
+
+    # end to end through the C ABI: host gate records in, <Z_i> + 1024 shots out
+    e2e_t = []
+    for i in range(max(2, min(args.steps, 3)) + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sv.reset()
+        sv.run(gates)
+        ez = sv.expectation_z_all()
+        outs = sv.sample(shots)
+        t1 = time.perf_counter()
+        if i > 0:
+            e2e_t.append(t1 - t0)
+    e2e_s = dist_max(statistics.median(e2e_t), ws)
+    h2d = gates.nbytes + shots.nbytes
+    d2h = ez.nbytes + outs.nbytes
+
+    # complex64 on the same circuit, and its fidelity against complex128
+    s64 = StateVector(n, "c64", device=local)
+    s64.set_timing(True)
+    t64 = []
+    for i in range(args.warmup + max(1, min(args.steps, 3))):
+        s64.reset()
+        s64.run(gates)
+        s64.flush()
+        st64 = s64.flush_stats()
+        if i >= args.warmup:
+            t64.append(st64["gpu_ms"] / 1e3)
+    c64_s = statistics.median(t64)
+    sv.reset()
+    sv.run(gates)
+    sv.synchronize()
+    a = torch.as_tensor(_DeviceView(sv.device_ptr(), 1 << n, "<c16"), device=f"cuda:{local}")
+    b = torch.as_tensor(_DeviceView(s64.device_ptr(), 1 << n, "<c8"), device=f"cuda:{local}")
+    fid = 0.0
+    maxerr = 0.0
+    chunk = 1 << 26
+    ip = torch.zeros((), dtype=torch.complex128, device=f"cuda:{local}")
+    for off in range(0, 1 << n, chunk):
+        bb = b[off:off + chunk].to(torch.complex128)
+        aa = a[off:off + chunk]
+        ip += torch.vdot(aa, bb)
+        maxerr = max(maxerr, float((aa - bb).abs().max().item()))
+    fid = float(ip.abs().item() ** 2)
+    s64.close()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            secs, sample, cores, kind = reference_sample(n, args.ref_budget, gates)
+            cpu = {"value": 1.0 / secs, "unit": "circuits/s", "cores": cores, "kind": kind, "sample": sample}
+        except Exception as e:  # reported, never silently replaced
+            cpu = {"value": None, "unit": "circuits/s", "cores": None, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ws / t_max, "unit": "circuits/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic seeded circuit (splitmix64 0xC2)",
+            "config": {"workload": WORKLOAD, "qubits": n, "depth": args.depth, "path": "plain c128 tiled",
+                       "parallelism": f"replicas x{ws}", "l2": "state (16 GiB) larger than L2",
+                       "tile_passes_per_circuit": passes, "gates": int(len(gates))},
+            "hbm_gbs_per_pass": achieved,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_tile<double>",
+                         "peak_source": peak_kind},
+            "c64": {"circuit_ms": c64_s * 1e3, "speedup_vs_c128": t_max / c64_s, "fidelity": fid,
+                    "max_amp_err": maxerr, "path": "c64 tiled"},
+            "e2e": {"value": ws / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sv.close()
+
+
+class _DeviceView:
+    """__cuda_array_interface__ over an engine-owned device buffer (for torch)."""
+
+    def __init__(self, ptr, count, typestr):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--depth", type=int, default=40)
+    ap.add_argument("--ref-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_b200(args, ws, rank, local)
+    finally:
+        dist_done(ws)
+
+
+if __name__ == "__main__":
+    main()

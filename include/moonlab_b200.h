@@ -1,0 +1,200 @@
+/*
+ * moonlab_b200.h -- C ABI of the B200 (sm_100a) dense state-vector engine.
+ *
+ * Plain C types only: pointers, sizes, integers, doubles.  Every entry point
+ * returns an mlb_status_t (0 = success, negative = error) unless stated.
+ * This is the engine's own surface; the reference-compatible drop-in symbols
+ * (quantum_state_create_gpu, qsim_gpu_route_*, moonlab_cuda_*,
+ * moonlab_vqe_gradient, the "b200" scheduler backend) are declared in
+ * moonlab_b200_dropin.h and are implemented on top of this one.
+ *
+ * State layout in HBM: 2^n amplitudes, interleaved (re, im), qubit 0 = the
+ * least-significant index bit -- the quantum_state_t.amplitudes layout of the
+ * reference (src/quantum/state.h:102-131).  complex128 states hold doubles,
+ * complex64 states floats.
+ *
+ * Threading: a state is not thread-safe (as quantum_state_t,
+ * src/quantum/state.h:98-100); distinct states may be used from distinct
+ * threads.  Gate calls are asynchronous: they are queued on the host and run
+ * on the state's stream in fused tile passes at the next read, flush or
+ * synchronize.
+ */
+#ifndef MOONLAB_B200_H
+#define MOONLAB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Everything declared here is exported from libmoonlab_b200.so (the library is
+ * built with -fvisibility=hidden). */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* Status codes.  0 .. -5 carry the meaning of moonlab_cuda_status_t
+ * (src/backends/cuda_statevec.h:39-46) so the drop-in layer passes them
+ * through unchanged. */
+typedef enum {
+    MLB_OK                = 0,
+    MLB_ERR_OUT_OF_MEMORY = -1,
+    MLB_ERR_NO_DEVICE     = -2,
+    MLB_ERR_DRIVER        = -3,
+    MLB_ERR_INVALID_QUBIT = -4,
+    MLB_ERR_NUM_QUBITS    = -5,
+    MLB_ERR_INVALID_ARG   = -6,
+    MLB_ERR_TIMEOUT       = -7,  /* a bounded device-side wait gave up */
+    MLB_ERR_BUSY          = -8,  /* admission refused (HBM budget / slots) */
+    MLB_ERR_NOT_SUPPORTED = -9
+} mlb_status_t;
+
+typedef enum { MLB_C128 = 0, MLB_C64 = 1 } mlb_dtype_t;
+
+/* Execution modes for queued gates. */
+typedef enum {
+    MLB_EXEC_TILED = 0,  /* default: gates grouped into shared-memory tile passes */
+    MLB_EXEC_EAGER = 1,  /* one full-state kernel per gate (the per-gate path) */
+    MLB_EXEC_FUSED = 2   /* complex64 states: gates fused into dense k<=5-qubit blocks */
+} mlb_exec_mode_t;
+
+/* Gate operation kinds understood by the engine (mlb_op_t.kind). */
+typedef enum {
+    MLB_OP_1Q      = 0, /* 2x2 matrix m[0..7] on target, if (idx & cmask) == cmask   */
+    MLB_OP_2Q      = 1, /* 4x4 matrix m[0..31] on (target = low bit, target2), cmask */
+    MLB_OP_DIAG1   = 2, /* diag(m[0]+i m[1], m[2]+i m[3]) on target, cmask           */
+    MLB_OP_X       = 3, /* swap the target pair where (idx & cmask) == cmask        */
+    MLB_OP_SWAP    = 4, /* swap bits target <-> target2 where cmask holds           */
+    MLB_OP_ZZ      = 5, /* amp *= (m[0],m[1]) if bit(target)==bit(target2) else (m[2],m[3]) */
+    MLB_OP_PHASE   = 6, /* amp *= (m[0],m[1]) where (idx & cmask) == cmask          */
+    MLB_OP_DENSE   = 7  /* dense 2^k x 2^k block (fused path); internal               */
+} mlb_op_kind_t;
+
+typedef struct {
+    int32_t  kind;
+    int32_t  target;
+    int32_t  target2;
+    int32_t  reserved;
+    uint64_t cmask;
+    double   m[32];
+} mlb_op_t;
+
+typedef struct mlb_state mlb_state_t;
+
+/* ---- device / lifecycle ---------------------------------------------- */
+int  mlb_device_count(int *count);
+int  mlb_state_create(uint32_t num_qubits, int dtype, int device, mlb_state_t **out);
+void mlb_state_free(mlb_state_t *s);
+int  mlb_state_num_qubits(const mlb_state_t *s, uint32_t *out);
+int  mlb_state_dim(const mlb_state_t *s, uint64_t *out);
+int  mlb_state_dtype(const mlb_state_t *s, int *out);
+int  mlb_state_device_ptr(mlb_state_t *s, void **out);   /* flushes first */
+int  mlb_state_set_stream(mlb_state_t *s, void *cuda_stream); /* NULL = own stream */
+int  mlb_state_stream(const mlb_state_t *s, void **cuda_stream); /* the stream kernels run on */
+int  mlb_state_set_exec_mode(mlb_state_t *s, int mode);
+int  mlb_state_reset(mlb_state_t *s);                     /* |0...0> */
+int  mlb_state_copy_to_host(mlb_state_t *s, void *host);  /* 2^n (re,im) of the dtype */
+int  mlb_state_copy_from_host(mlb_state_t *s, const void *host);
+int  mlb_state_copy(mlb_state_t *dst, mlb_state_t *src); /* same n; dtype may differ */
+int  mlb_flush(mlb_state_t *s);
+int  mlb_synchronize(mlb_state_t *s);
+
+/* ---- gates (queued) ---------------------------------------------------- */
+int  mlb_apply_op(mlb_state_t *s, const mlb_op_t *op);
+int  mlb_apply_ops(mlb_state_t *s, const mlb_op_t *ops, size_t num_ops);
+int  mlb_apply_1q(mlb_state_t *s, uint32_t target, const double m[8]);
+int  mlb_apply_2q(mlb_state_t *s, uint32_t q0, uint32_t q1, const double m[32]);
+int  mlb_apply_controlled_1q(mlb_state_t *s, uint64_t control_mask, uint32_t target,
+                             const double m[8]);
+int  mlb_apply_mcx(mlb_state_t *s, uint64_t control_mask, uint32_t target);
+int  mlb_apply_mcz(mlb_state_t *s, uint64_t all_mask);
+int  mlb_apply_swap(mlb_state_t *s, uint64_t control_mask, uint32_t q0, uint32_t q1);
+int  mlb_apply_zz(mlb_state_t *s, uint32_t q0, uint32_t q1, double theta);
+
+/* ---- FP64 reductions (one HBM pass each) ------------------------------- */
+int  mlb_norm_sq(mlb_state_t *s, double *out);
+int  mlb_prob_one(mlb_state_t *s, uint32_t qubit, double *out);
+int  mlb_prob_one_all(mlb_state_t *s, double *out_n);          /* P1 of every qubit */
+int  mlb_expect_z_all(mlb_state_t *s, double *out_n);          /* 1 - 2 P1 */
+/* P(qubit = 1) bit-identical to measurement_probability_one (measurement.c:73):
+ * the reference's left-to-right fused sum, reproduced exactly (two passes). */
+int  mlb_prob_one_exact(mlb_state_t *s, uint32_t qubit, double *out);
+int  mlb_correlation_zz(mlb_state_t *s, uint32_t q1, uint32_t q2, double *out);
+int  mlb_expect_pauli(mlb_state_t *s, uint64_t xmask, uint64_t zmask, double *out);
+int  mlb_expect_pauli_sum(mlb_state_t *s, size_t num_terms, const uint64_t *xmasks,
+                          const uint64_t *zmasks, const double *coeffs, double *out);
+/* probability vector; rule 0 = cabs(a)^2 (measurement.c:140),
+ * rule 1 = re*re + im*im (moonlab_qgtl_backend.c:199-210).
+ * out_host may be NULL when out_device is given (device pointer, 2^n doubles). */
+int  mlb_probabilities(mlb_state_t *s, int rule, double *out_host, void *out_device);
+
+/* ---- sampling and collapse (bit-exact vs the reference given uniforms) -- */
+enum { MLB_SAMPLE_CDF_GE = 0,   /* measurement_sample: first i with cdf_i >= u      */
+       MLB_SAMPLE_CUM_GT = 1 }; /* measurement_all_qubits: first i with u < cum_i  */
+int  mlb_sample(mlb_state_t *s, int rule, const double *uniforms, size_t num,
+                uint64_t *outcomes);
+/* measurement_single_qubit semantics; *outcome = -1 when the kept norm is tiny */
+int  mlb_measure_qubit(mlb_state_t *s, uint32_t qubit, double u, int *outcome);
+/* quantum_measure (computational basis) semantics */
+int  mlb_quantum_measure(mlb_state_t *s, uint32_t qubit, double u, int *outcome,
+                         double *probability);
+/* measurement_all_qubits: sample (rule CUM_GT) and collapse to the basis state */
+int  mlb_measure_all(mlb_state_t *s, double u, uint64_t *outcome);
+int  mlb_normalize(mlb_state_t *s, double *norm_out);
+
+/* ---- circuits ------------------------------------------------------------ */
+/* Circuit gate record.  type: the QGTL gate enum 0..13
+ * (moonlab_qgtl_backend.h:57-72; CY composed as S.CNOT.Sdg like
+ * moonlab_qgtl_backend.c:138-144) plus Sdg = 20, Tdg = 21, Phase = 22,
+ * CPhase = 23, CRX = 24, CRY = 25, CRZ = 26 (gates.c:345-887) and
+ * ZZ(theta) = 27 (exp(-i theta/2 Z Z), qaoa.c:745-753).  Two-qubit records
+ * use `control` as the control (or first qubit) and `target` as the target. */
+typedef struct {
+    int32_t type;
+    int32_t target;
+    int32_t control;   /* control (CNOT/CY/CZ), qubit1 (SWAP), second qubit (ZZ) */
+    int32_t reserved;
+    double  theta;
+} mlb_gate_t;
+enum { MLB_GATE_SDG = 20, MLB_GATE_TDG = 21, MLB_GATE_PHASE = 22, MLB_GATE_CPHASE = 23,
+       MLB_GATE_CRX = 24, MLB_GATE_CRY = 25, MLB_GATE_CRZ = 26, MLB_GATE_ZZ = 27 };
+
+/* Translate gate records into engine ops exactly as the reference's gate_*
+ * functions build their GPU-route matrices (host libm cos/sin/cexp). */
+int  mlb_gates_to_ops(const mlb_gate_t *gates, size_t num_gates, uint32_t num_qubits,
+                      mlb_op_t *ops_out, size_t *num_ops_out);
+int  mlb_run_gates(mlb_state_t *s, const mlb_gate_t *gates, size_t num_gates);
+
+/* Plan statistics of the last flush: passes launched and ops applied. */
+typedef struct {
+    uint64_t passes;
+    uint64_t ops;
+    uint64_t dense_blocks;
+    uint64_t bytes_moved;    /* algorithmic HBM bytes of the launched passes */
+    uint64_t kernel_launches;
+    double   gpu_ms;         /* device time of the flush's kernels (timing enabled), else 0 */
+} mlb_flush_stats_t;
+int  mlb_last_flush_stats(mlb_state_t *s, mlb_flush_stats_t *out);
+/* Record CUDA events around each flush's kernels on the state's stream;
+ * mlb_last_flush_stats then reports their elapsed device time (synchronizes). */
+int  mlb_state_set_timing(mlb_state_t *s, int enable);
+/* Plan ops exactly as a flush would, on the host only (no device needed):
+ * reports the passes and algorithmic bytes a flush of these ops launches. */
+int  mlb_plan_ops(const mlb_op_t *ops, size_t num_ops, uint32_t num_qubits, int dtype,
+                  int fuse1q, mlb_flush_stats_t *out);
+int  mlb_total_kernel_launches(uint64_t *out);
+
+/* ---- error text ---------------------------------------------------------- */
+const char *mlb_status_string(int status);
+const char *mlb_last_error(void);   /* thread-local detail of the last failure */
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOONLAB_B200_H */

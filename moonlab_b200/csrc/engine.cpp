@@ -1,0 +1,1355 @@
+// engine.cpp -- host runtime of the B200 state-vector engine and its C ABI
+// (include/moonlab_b200.h).
+//
+// A state owns its HBM buffer, a CUDA stream and a host-side queue of gate
+// ops.  Gate calls only validate, canonicalise and queue; the queue is
+// flushed at the next read, synchronize or explicit flush.  A flush lowers
+// the queue into tile passes (kernels_tile.cu): the planner greedily picks
+// the high qubits of each pass so that as many queued ops as possible run
+// in one read+write of the state, keeping program order between ops that
+// share a qubit.  Controls and diagonal qubits never need to be inside a
+// tile (they are constant over it), so CNOT ladders and ZZ layers cost no
+// tile room for their controls / phases.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "mlb_internal.h"
+
+extern "C" {
+void mlb_mat_rx(double theta, double m[8]);
+void mlb_mat_ry(double theta, double m[8]);
+void mlb_mat_rz(double theta, double m[8]);
+void mlb_mat_phase1(int which, double theta, double m[8]);
+void mlb_mat_zz(double theta, double out[4]);
+void mlb_mat_cphase(double theta, double out[2]);
+void mlb_mat_crz_inner(double theta, double m[8]);
+}
+
+namespace mlb {
+static std::atomic<uint64_t> g_launches{0};
+uint64_t kernel_launch_count() { return g_launches.load(); }
+void count_launch(uint64_t k) { g_launches.fetch_add(k); }
+}  // namespace mlb
+
+using namespace mlb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? MLB_ERR_OUT_OF_MEMORY : MLB_ERR_DRIVER, "%s: %s", what,
+              cudaGetErrorString(e));
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+inline int popc(uint64_t x) { return __builtin_popcountll(x); }
+
+// Tile geometry per dtype (must match TileCfg in kernels_tile.cu).
+struct Geo {
+  int TB, RB;
+};
+inline Geo geo(int dtype) { return dtype == MLB_C128 ? Geo{12, 3} : Geo{13, 4}; }
+
+}  // namespace
+
+struct mlb_state {
+  uint32_t n = 0;
+  int dtype = MLB_C128;
+  int device = 0;
+  void* amp = nullptr;
+  size_t bytes = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  int mode = MLB_EXEC_TILED;
+  bool fuse1q = true;
+  int num_sms = 148;
+  std::vector<mlb_op_t> queue;
+  // device scratch for reductions
+  double* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  // plan upload buffers
+  void* d_plan = nullptr;
+  size_t d_plan_bytes = 0;
+  void* h_plan = nullptr;
+  size_t h_plan_bytes = 0;
+  cudaEvent_t plan_ev = nullptr;
+  bool plan_ev_pending = false;
+  bool timing = false;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  bool timed_pending = false;
+  mlb_flush_stats_t stats{};
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// op validation and canonicalisation
+// ---------------------------------------------------------------------------
+bool is_zero(const double* m, int k) { return m[2 * k] == 0.0 && m[2 * k + 1] == 0.0; }
+bool is_one(const double* m, int k) { return m[2 * k] == 1.0 && m[2 * k + 1] == 0.0; }
+
+uint64_t op_targets(const mlb_op_t& o) {
+  switch (o.kind) {
+    case MLB_OP_1Q:
+    case MLB_OP_X: return 1ull << o.target;
+    case MLB_OP_2Q:
+    case MLB_OP_SWAP: return (1ull << o.target) | (1ull << o.target2);
+    default: return 0;  // diagonal
+  }
+}
+uint64_t op_qubits(const mlb_op_t& o) {
+  uint64_t q = o.cmask | op_targets(o);
+  if (o.kind == MLB_OP_DIAG1) q |= 1ull << o.target;
+  if (o.kind == MLB_OP_ZZ) q |= (1ull << o.target) | (1ull << o.target2);
+  return q;
+}
+
+int validate(const mlb_state* s, const mlb_op_t& o) {
+  const uint32_t n = s->n;
+  const uint64_t all = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+  auto bad_q = [&](int q) { return q < 0 || (uint32_t)q >= n; };
+  if (o.cmask & ~all) return fail(MLB_ERR_INVALID_QUBIT, "control mask outside the register");
+  switch (o.kind) {
+    case MLB_OP_1Q:
+    case MLB_OP_X:
+    case MLB_OP_DIAG1:
+      if (bad_q(o.target)) return fail(MLB_ERR_INVALID_QUBIT, "target %d out of range", o.target);
+      if (o.cmask >> o.target & 1ull) return fail(MLB_ERR_INVALID_QUBIT, "target in control mask");
+      return MLB_OK;
+    case MLB_OP_2Q:
+    case MLB_OP_SWAP:
+    case MLB_OP_ZZ:
+      if (bad_q(o.target) || bad_q(o.target2))
+        return fail(MLB_ERR_INVALID_QUBIT, "qubits (%d,%d) out of range", o.target, o.target2);
+      if (o.target == o.target2) return fail(MLB_ERR_INVALID_QUBIT, "repeated qubit %d", o.target);
+      if ((o.cmask >> o.target & 1ull) || (o.cmask >> o.target2 & 1ull))
+        return fail(MLB_ERR_INVALID_QUBIT, "target in control mask");
+      return MLB_OK;
+    case MLB_OP_PHASE:
+      if (o.cmask == 0) return fail(MLB_ERR_INVALID_ARG, "phase op with empty mask");
+      return MLB_OK;
+    default:
+      return fail(MLB_ERR_INVALID_ARG, "unknown op kind %d", o.kind);
+  }
+}
+
+// Rewrite an op into the cheapest equivalent kind.  Matrices are only
+// re-labelled, never re-computed, so values stay bit-identical.
+mlb_op_t canonical(const mlb_op_t& in) {
+  mlb_op_t o = in;
+  if (o.kind == MLB_OP_1Q) {
+    const double* m = o.m;
+    if (is_zero(m, 1) && is_zero(m, 2)) {  // diagonal
+      mlb_op_t d{};
+      d.kind = MLB_OP_DIAG1;
+      d.target = o.target;
+      d.target2 = -1;
+      d.cmask = o.cmask;
+      d.m[0] = m[0]; d.m[1] = m[1]; d.m[2] = m[6]; d.m[3] = m[7];
+      if (is_one(d.m, 0)) {  // phase on the |1> half only
+        mlb_op_t p{};
+        p.kind = MLB_OP_PHASE;
+        p.target = o.target;
+        p.target2 = -1;
+        p.cmask = o.cmask | (1ull << o.target);
+        p.m[0] = m[6]; p.m[1] = m[7];
+        return p;
+      }
+      return d;
+    }
+    if (is_zero(m, 0) && is_zero(m, 3) && is_one(m, 1) && is_one(m, 2)) {
+      mlb_op_t x{};
+      x.kind = MLB_OP_X;
+      x.target = o.target;
+      x.target2 = -1;
+      x.cmask = o.cmask;
+      return x;
+    }
+    return o;
+  }
+  if (o.kind == MLB_OP_2Q) {
+    const double* m = o.m;  // m[(r*4+c)*2]
+    auto E = [&](int r, int c) { return r * 4 + c; };
+    bool diag = true;
+    for (int r = 0; r < 4; r++)
+      for (int c = 0; c < 4; c++)
+        if (r != c && !is_zero(m, E(r, c))) diag = false;
+    const int q0 = o.target, q1 = o.target2;
+    if (diag) {
+      if (is_one(m, E(0, 0)) && is_one(m, E(1, 1)) && is_one(m, E(2, 2))) {
+        mlb_op_t p{};
+        p.kind = MLB_OP_PHASE;
+        p.target = q0;
+        p.target2 = q1;
+        p.cmask = o.cmask | (1ull << q0) | (1ull << q1);
+        p.m[0] = m[2 * E(3, 3)]; p.m[1] = m[2 * E(3, 3) + 1];
+        return p;
+      }
+      const double* a = &m[2 * E(0, 0)];
+      const double* b = &m[2 * E(1, 1)];
+      const double* c = &m[2 * E(2, 2)];
+      const double* d = &m[2 * E(3, 3)];
+      if (a[0] == d[0] && a[1] == d[1] && b[0] == c[0] && b[1] == c[1] && o.cmask == 0) {
+        mlb_op_t z{};
+        z.kind = MLB_OP_ZZ;
+        z.target = q0;
+        z.target2 = q1;
+        z.m[0] = a[0]; z.m[1] = a[1]; z.m[2] = b[0]; z.m[3] = b[1];
+        return z;
+      }
+    }
+    // SWAP permutation
+    bool swp = true;
+    for (int r = 0; r < 4; r++)
+      for (int c = 0; c < 4; c++) {
+        const int want = (r == 0 && c == 0) || (r == 3 && c == 3) || (r == 1 && c == 2) || (r == 2 && c == 1);
+        if (want ? !is_one(m, E(r, c)) : !is_zero(m, E(r, c))) swp = false;
+      }
+    if (swp) {
+      mlb_op_t w{};
+      w.kind = MLB_OP_SWAP;
+      w.target = q0;
+      w.target2 = q1;
+      w.cmask = o.cmask;
+      return w;
+    }
+    // controlled-1q with control q0 (identity on the q0 = 0 sector, rows/cols 0 and 2)
+    auto ctrl_form = [&](int i0, int i1, int j0, int j1) {
+      // identity on indices i0,i1; zero couplings between {i0,i1} and {j0,j1}
+      if (!is_one(m, E(i0, i0)) || !is_one(m, E(i1, i1))) return false;
+      if (!is_zero(m, E(i0, i1)) || !is_zero(m, E(i1, i0))) return false;
+      const int I[2] = {i0, i1}, J[2] = {j0, j1};
+      for (int a2 = 0; a2 < 2; a2++)
+        for (int b2 = 0; b2 < 2; b2++)
+          if (!is_zero(m, E(I[a2], J[b2])) || !is_zero(m, E(J[b2], I[a2]))) return false;
+      return true;
+    };
+    if (ctrl_form(0, 2, 1, 3)) {  // control q0, target q1, U from rows/cols {1,3}
+      mlb_op_t u{};
+      u.kind = MLB_OP_1Q;
+      u.target = q1;
+      u.target2 = -1;
+      u.cmask = o.cmask | (1ull << q0);
+      const int idx[4] = {E(1, 1), E(1, 3), E(3, 1), E(3, 3)};
+      for (int k = 0; k < 4; k++) { u.m[2 * k] = m[2 * idx[k]]; u.m[2 * k + 1] = m[2 * idx[k] + 1]; }
+      return canonical(u);
+    }
+    if (ctrl_form(0, 1, 2, 3)) {  // control q1, target q0, U from rows/cols {2,3}
+      mlb_op_t u{};
+      u.kind = MLB_OP_1Q;
+      u.target = q0;
+      u.target2 = -1;
+      u.cmask = o.cmask | (1ull << q1);
+      const int idx[4] = {E(2, 2), E(2, 3), E(3, 2), E(3, 3)};
+      for (int k = 0; k < 4; k++) { u.m[2 * k] = m[2 * idx[k]]; u.m[2 * k + 1] = m[2 * idx[k] + 1]; }
+      return canonical(u);
+    }
+    return o;
+  }
+  if (o.kind == MLB_OP_DIAG1 && is_one(o.m, 0)) {
+    mlb_op_t p{};
+    p.kind = MLB_OP_PHASE;
+    p.target = o.target;
+    p.target2 = -1;
+    p.cmask = o.cmask | (1ull << o.target);
+    p.m[0] = o.m[2]; p.m[1] = o.m[3];
+    return p;
+  }
+  return o;
+}
+
+// Single-qubit op as a 2x2 matrix (for run fusion); false if not 1q-uncontrolled.
+bool as_2x2(const mlb_op_t& o, double m[8]) {
+  if (o.cmask != 0) {
+    if (!(o.kind == MLB_OP_PHASE && popc(o.cmask) == 1)) return false;
+  }
+  switch (o.kind) {
+    case MLB_OP_1Q: std::memcpy(m, o.m, 8 * sizeof(double)); return true;
+    case MLB_OP_X: { const double x[8] = {0, 0, 1, 0, 1, 0, 0, 0}; std::memcpy(m, x, sizeof x); return true; }
+    case MLB_OP_DIAG1: { const double d[8] = {o.m[0], o.m[1], 0, 0, 0, 0, o.m[2], o.m[3]}; std::memcpy(m, d, sizeof d); return true; }
+    case MLB_OP_PHASE: { const double d[8] = {1, 0, 0, 0, 0, 0, o.m[0], o.m[1]}; std::memcpy(m, d, sizeof d); return true; }
+    default: return false;
+  }
+}
+int single_qubit_of(const mlb_op_t& o) {
+  if (o.kind == MLB_OP_PHASE) return popc(o.cmask) == 1 ? __builtin_ctzll(o.cmask) : -1;
+  if (o.cmask) return -1;
+  if (o.kind == MLB_OP_1Q || o.kind == MLB_OP_X || o.kind == MLB_OP_DIAG1) return o.target;
+  return -1;
+}
+
+// m = b * a (apply a first, then b)
+void mul2(const double b[8], const double a[8], double out[8]) {
+  for (int r = 0; r < 2; r++)
+    for (int c = 0; c < 2; c++) {
+      double re = 0, im = 0;
+      for (int k = 0; k < 2; k++) {
+        const double br = b[(r * 2 + k) * 2], bi = b[(r * 2 + k) * 2 + 1];
+        const double ar = a[(k * 2 + c) * 2], ai = a[(k * 2 + c) * 2 + 1];
+        re += br * ar - bi * ai;
+        im += br * ai + bi * ar;
+      }
+      out[(r * 2 + c) * 2] = re;
+      out[(r * 2 + c) * 2 + 1] = im;
+    }
+}
+
+// Merge runs of uncontrolled single-qubit ops on the same qubit into one
+// 2x2 (the FUSED_1Q rule of fuse_compile, fusion.c:247-292).
+std::vector<mlb_op_t> fuse_1q_runs(const std::vector<mlb_op_t>& in, uint32_t n) {
+  std::vector<mlb_op_t> out;
+  out.reserve(in.size());
+  std::vector<long> open(n, -1);  // index in out of the open 1q op per qubit
+  for (const auto& o : in) {
+    const int q = single_qubit_of(o);
+    if (q >= 0 && open[q] >= 0) {
+      double a[8], b[8], r[8];
+      as_2x2(out[open[q]], a);
+      as_2x2(o, b);
+      mul2(b, a, r);
+      mlb_op_t f{};
+      f.kind = MLB_OP_1Q;
+      f.target = q;
+      f.target2 = -1;
+      std::memcpy(f.m, r, sizeof r);
+      out[open[q]] = f;
+      continue;
+    }
+    const uint64_t qs = op_qubits(o);
+    for (uint32_t b = 0; b < n; b++)
+      if (qs >> b & 1ull) open[b] = -1;
+    out.push_back(o);
+    if (q >= 0) open[q] = (long)out.size() - 1;
+  }
+  for (auto& o : out)
+    if (o.kind == MLB_OP_1Q) o = canonical(o);
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// planner
+// ---------------------------------------------------------------------------
+struct PlannedPass {
+  DevPass pass;
+  int seg_begin, seg_end;
+};
+
+struct Planner {
+  uint32_t n;
+  int dtype;
+  Geo g;
+  std::vector<PlannedPass> passes;
+  std::vector<DevSegment> segs;
+  std::vector<DevOp> dops;
+
+  // Choose the ops of one pass from `rem` (indices into ops), program order.
+  // Returns taken indices; fills high mask.
+  std::vector<int> choose(const std::vector<mlb_op_t>& ops, const std::vector<int>& rem, int L,
+                          uint64_t& SH_out) {
+    const uint64_t lowm = (1ull << L) - 1ull;
+    const int Hmax = g.TB - L;
+    const uint64_t allm = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+    // strategy A: first come
+    auto run = [&](uint64_t SH, bool grow, std::vector<int>* taken) {
+      uint64_t blocked = 0;
+      int cnt = 0;
+      for (int idx : rem) {
+        const mlb_op_t& o = ops[idx];
+        const uint64_t Q = op_qubits(o), T = op_targets(o);
+        if (Q & blocked) { blocked |= Q; if (blocked == allm) break; continue; }
+        const uint64_t need = T & ~lowm & ~SH;
+        if (need == 0 || (grow && popc(SH | need) <= Hmax)) {
+          SH |= need;
+          cnt++;
+          if (taken) taken->push_back(idx);
+        } else {
+          blocked |= Q;
+          if (blocked == allm) break;
+        }
+      }
+      return std::make_pair(cnt, SH);
+    };
+    auto A = run(0, true, nullptr);
+    // strategy B: the Hmax high qubits most demanded by the first ops
+    std::vector<double> score(n, 0.0);
+    {
+      int seen = 0;
+      for (int idx : rem) {
+        const uint64_t T = op_targets(ops[idx]) & ~lowm;
+        for (uint32_t b = 0; b < n; b++)
+          if (T >> b & 1ull) score[b] += 1.0 / (1.0 + seen * 0.02);
+        if (++seen > 8 * (int)n) break;
+      }
+    }
+    std::vector<int> order;
+    for (uint32_t b = L; b < n; b++) order.push_back((int)b);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return score[a] > score[b]; });
+    uint64_t SHB = 0;
+    for (int k = 0; k < (int)order.size() && k < Hmax; k++)
+      if (score[order[k]] > 0) SHB |= 1ull << order[k];
+    auto B = run(SHB, true, nullptr);
+    std::vector<int> taken;
+    if (B.first > A.first) {
+      run(SHB, true, &taken);
+      SH_out = B.second;
+    } else {
+      run(0, true, &taken);
+      SH_out = A.second;
+    }
+    return taken;
+  }
+
+  void lower_pass(const std::vector<mlb_op_t>& ops, const std::vector<int>& taken, int L, uint64_t SH) {
+    PlannedPass pp{};
+    DevPass& P = pp.pass;
+    P.n = (int)n;
+    P.L = L;
+    int local_of[64];
+    for (int q = 0; q < 64; q++) local_of[q] = -1;
+    for (int q = 0; q < L; q++) local_of[q] = q;
+    int H = 0;
+    for (uint32_t q = L; q < n; q++)
+      if (SH >> q & 1ull) {
+        P.high[H] = (int)q;
+        local_of[q] = L + H;
+        H++;
+      }
+    P.H = H;
+    const int m = L + H;
+    const uint64_t allm = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+    P.tile_free_mask = allm & ~(((1ull << L) - 1ull) | SH);
+    P.num_tiles = 1ull << (n - m);
+    const int RB = std::min(g.RB, m);
+    pp.seg_begin = (int)segs.size();
+
+    auto local_mask = [&](uint64_t gm, uint32_t& lm, uint64_t& om) {
+      lm = 0;
+      om = 0;
+      for (uint32_t b = 0; b < n; b++)
+        if (gm >> b & 1ull) {
+          if (local_of[b] >= 0) lm |= 1u << local_of[b];
+          else om |= 1ull << b;
+        }
+    };
+    size_t i = 0;
+    while (i < taken.size()) {
+      // grow a segment
+      uint32_t bits = 0;
+      size_t j = i;
+      for (; j < taken.size(); j++) {
+        const uint64_t T = op_targets(ops[taken[j]]);
+        uint32_t tl = 0;
+        uint64_t dummy;
+        local_mask(T, tl, dummy);
+        if (popc(bits | tl) > RB) break;
+        bits |= tl;
+      }
+      // pad to RB bits with the lowest free local bits
+      for (int b = 0; b < m && popc(bits) < RB; b++) bits |= 1u << b;
+      DevSegment sg{};
+      sg.nbits = 0;
+      for (int b = 0; b < m; b++)
+        if (bits >> b & 1u) sg.bits[sg.nbits++] = b;
+      auto rpos = [&](int lbit) {
+        for (int k = 0; k < sg.nbits; k++)
+          if (sg.bits[k] == lbit) return k;
+        return -1;
+      };
+      sg.op_begin = (int)dops.size();
+      for (size_t k = i; k < j; k++) {
+        const mlb_op_t& o = ops[taken[k]];
+        DevOp d{};
+        std::memcpy(d.m, o.m, sizeof d.m);
+        local_mask(o.cmask, d.lcmask, d.ocmask);
+        d.lt = -1;
+        switch (o.kind) {
+          case MLB_OP_1Q: {
+            bool real = true;
+            for (int t = 1; t < 8; t += 2)
+              if (o.m[t] != 0.0) real = false;
+            d.kind = real ? DOP_1Q_REAL : DOP_1Q_GEN;
+            d.rt = rpos(local_of[o.target]);
+            break;
+          }
+          case MLB_OP_X: d.kind = DOP_X; d.rt = rpos(local_of[o.target]); break;
+          case MLB_OP_2Q:
+          case MLB_OP_SWAP:
+            d.kind = o.kind == MLB_OP_2Q ? DOP_2Q_GEN : DOP_SWAP;
+            d.rt = rpos(local_of[o.target]);
+            d.rt2 = rpos(local_of[o.target2]);
+            break;
+          case MLB_OP_DIAG1:
+            d.kind = DOP_DIAG1;
+            d.lt = local_of[o.target];
+            d.omask = d.lt >= 0 ? 0 : (1ull << o.target);
+            break;
+          case MLB_OP_PHASE: {
+            d.kind = DOP_PHASE;
+            local_mask(o.cmask, d.lmask, d.omask);
+            d.lcmask = 0;
+            d.ocmask = 0;
+            break;
+          }
+          case MLB_OP_ZZ: {
+            d.kind = DOP_ZZ;
+            local_mask((1ull << o.target) | (1ull << o.target2), d.lmask, d.omask);
+            break;
+          }
+        }
+        dops.push_back(d);
+      }
+      sg.op_end = (int)dops.size();
+      segs.push_back(sg);
+      i = j;
+    }
+    pp.seg_end = (int)segs.size();
+    P.num_segments = pp.seg_end - pp.seg_begin;
+    passes.push_back(pp);
+  }
+
+  void plan(const std::vector<mlb_op_t>& ops) {
+    std::vector<int> rem(ops.size());
+    for (size_t i = 0; i < ops.size(); i++) rem[i] = (int)i;
+    const int L = (int)n <= g.TB ? (int)n : 5;
+    while (!rem.empty()) {
+      uint64_t SH = 0;
+      std::vector<int> taken;
+      if ((int)n <= g.TB) {
+        taken = rem;
+      } else {
+        taken = choose(ops, rem, L, SH);
+      }
+      lower_pass(ops, taken, L, SH);
+      // remove taken (both lists ascending)
+      std::vector<int> next;
+      next.reserve(rem.size() - taken.size());
+      size_t t = 0;
+      for (int idx : rem) {
+        if (t < taken.size() && taken[t] == idx) { t++; continue; }
+        next.push_back(idx);
+      }
+      rem.swap(next);
+    }
+  }
+};
+
+int ensure_scratch(mlb_state* s, size_t bytes) {
+  if (s->scratch_bytes >= bytes) return MLB_OK;
+  if (s->d_scratch) {
+    cudaStreamSynchronize(s->stream);
+    cudaFree(s->d_scratch);
+    s->d_scratch = nullptr;
+    s->scratch_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc((void**)&s->d_scratch, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "scratch allocation");
+  s->scratch_bytes = bytes;
+  return MLB_OK;
+}
+
+int upload_plan(mlb_state* s, const void* host, size_t bytes) {
+  if (s->plan_ev_pending) {
+    cudaEventSynchronize(s->plan_ev);
+    s->plan_ev_pending = false;
+  }
+  if (s->h_plan_bytes < bytes) {
+    if (s->h_plan) cudaFreeHost(s->h_plan);
+    s->h_plan = nullptr;
+    size_t nb = std::max(bytes, (size_t)1 << 20);
+    cudaError_t e = cudaMallocHost(&s->h_plan, nb);
+    if (e != cudaSuccess) { s->h_plan_bytes = 0; return cuda_fail(e, "pinned plan buffer"); }
+    s->h_plan_bytes = nb;
+  }
+  if (s->d_plan_bytes < bytes) {
+    if (s->d_plan) { cudaStreamSynchronize(s->stream); cudaFree(s->d_plan); }
+    s->d_plan = nullptr;
+    size_t nb = std::max(bytes, (size_t)1 << 20);
+    cudaError_t e = cudaMalloc(&s->d_plan, nb);
+    if (e != cudaSuccess) { s->d_plan_bytes = 0; return cuda_fail(e, "device plan buffer"); }
+    s->d_plan_bytes = nb;
+  }
+  std::memcpy(s->h_plan, host, bytes);
+  cudaError_t e = cudaMemcpyAsync(s->d_plan, s->h_plan, bytes, cudaMemcpyHostToDevice, s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "plan upload");
+  cudaEventRecord(s->plan_ev, s->stream);
+  s->plan_ev_pending = true;
+  return MLB_OK;
+}
+
+int flush_impl(mlb_state* s) {
+  if (s->queue.empty()) return MLB_OK;
+  DeviceGuard dg(s->device);
+  mlb_flush_stats_t st{};
+  const uint64_t dim = 1ull << s->n;
+  const uint64_t ab = s->dtype == MLB_C128 ? 16 : 8;
+  if (s->mode == MLB_EXEC_EAGER) {
+    if (s->timing) cudaEventRecord(s->t0, s->stream);
+    for (const auto& o : s->queue) {
+      int rc = launch_gate(s->dtype, s->amp, (int)s->n, o, s->stream);
+      if (rc) { s->queue.clear(); return fail(rc, "gate launch failed: %s", cudaGetErrorString(cudaGetLastError())); }
+      st.ops++;
+      st.passes++;
+      st.kernel_launches++;
+      const int c = popc(o.cmask);
+      uint64_t touched = dim >> c;
+      if (o.kind == MLB_OP_PHASE) touched = dim >> popc(o.cmask);
+      st.bytes_moved += 2 * ab * touched;
+    }
+    s->queue.clear();
+    if (s->timing) {
+      cudaEventRecord(s->t1, s->stream);
+      s->timed_pending = true;
+    }
+    s->stats = st;
+    return MLB_OK;
+  }
+  std::vector<mlb_op_t> ops = s->fuse1q ? fuse_1q_runs(s->queue, s->n) : s->queue;
+  s->queue.clear();
+  Planner pl{s->n, s->dtype, geo(s->dtype), {}, {}, {}};
+  pl.plan(ops);
+  // one upload: ops then segments
+  const size_t ob = pl.dops.size() * sizeof(DevOp);
+  const size_t sb = pl.segs.size() * sizeof(DevSegment);
+  std::vector<unsigned char> blob(ob + sb + 16);
+  std::memcpy(blob.data(), pl.dops.data(), ob);
+  size_t soff = (ob + 15) & ~(size_t)15;
+  std::memcpy(blob.data() + soff, pl.segs.data(), sb);
+  int rc = upload_plan(s, blob.data(), soff + sb);
+  if (rc) return rc;
+  const DevOp* d_ops = reinterpret_cast<const DevOp*>(s->d_plan);
+  const DevSegment* d_segs = reinterpret_cast<const DevSegment*>((unsigned char*)s->d_plan + soff);
+  if (s->timing) cudaEventRecord(s->t0, s->stream);
+  for (const auto& pp : pl.passes) {
+    rc = launch_tile_pass(s->dtype, s->amp, pp.pass, d_segs + pp.seg_begin, d_ops, nullptr, s->num_sms,
+                          s->stream);
+    if (rc) return fail(rc, "tile pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    st.passes++;
+    st.kernel_launches++;
+    st.bytes_moved += 2 * ab * dim;
+  }
+  st.ops = ops.size();
+  if (s->timing) {
+    cudaEventRecord(s->t1, s->stream);
+    s->timed_pending = true;
+  }
+  s->stats = st;
+  return MLB_OK;
+}
+
+int enqueue(mlb_state* s, const mlb_op_t& op) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  int rc = validate(s, op);
+  if (rc) return rc;
+  s->queue.push_back(canonical(op));
+  if (s->queue.size() >= 65536) return flush_impl(s);
+  return MLB_OK;
+}
+
+int sync_stream(mlb_state* s) {
+  cudaError_t e = cudaStreamSynchronize(s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
+  return MLB_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* mlb_status_string(int st) {
+  switch (st) {
+    case MLB_OK: return "ok";
+    case MLB_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case MLB_ERR_NO_DEVICE: return "no CUDA device";
+    case MLB_ERR_DRIVER: return "CUDA driver/runtime error";
+    case MLB_ERR_INVALID_QUBIT: return "invalid qubit";
+    case MLB_ERR_NUM_QUBITS: return "unsupported number of qubits";
+    case MLB_ERR_INVALID_ARG: return "invalid argument";
+    case MLB_ERR_TIMEOUT: return "device wait timed out";
+    case MLB_ERR_BUSY: return "admission refused";
+    case MLB_ERR_NOT_SUPPORTED: return "not supported";
+    default: return "unknown status";
+  }
+}
+
+const char* mlb_last_error(void) { return g_err.c_str(); }
+
+int mlb_device_count(int* count) {
+  if (!count) return fail(MLB_ERR_INVALID_ARG, "null count");
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    *count = 0;
+    cudaGetLastError();
+    return fail(MLB_ERR_NO_DEVICE, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+  }
+  *count = c;
+  return MLB_OK;
+}
+
+int mlb_state_create(uint32_t n, int dtype, int device, mlb_state_t** out) {
+  if (!out) return fail(MLB_ERR_INVALID_ARG, "null out");
+  *out = nullptr;
+  if (dtype != MLB_C128 && dtype != MLB_C64) return fail(MLB_ERR_INVALID_ARG, "bad dtype %d", dtype);
+  const uint32_t maxq = dtype == MLB_C128 ? 33 : 34;
+  if (n < 1 || n > maxq) return fail(MLB_ERR_NUM_QUBITS, "num_qubits %u outside [1, %u]", n, maxq);
+  int cnt = 0;
+  if (mlb_device_count(&cnt) != MLB_OK || cnt == 0) return fail(MLB_ERR_NO_DEVICE, "no CUDA device visible");
+  if (device < 0 || device >= cnt) return fail(MLB_ERR_NO_DEVICE, "device %d of %d", device, cnt);
+  DeviceGuard dg(device);
+  auto* s = new (std::nothrow) mlb_state();
+  if (!s) return fail(MLB_ERR_OUT_OF_MEMORY, "host allocation");
+  s->n = n;
+  s->dtype = dtype;
+  s->device = device;
+  s->bytes = (size_t)(dtype == MLB_C128 ? 16 : 8) << n;
+  cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
+  cudaError_t e = cudaMalloc(&s->amp, s->bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete s;
+    return cuda_fail(e, "state allocation");
+  }
+  e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->plan_ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    cudaFree(s->amp);
+    delete s;
+    return cuda_fail(e, "stream creation");
+  }
+  int rc = launch_init_zero(dtype, s->amp, (int)n, s->stream);
+  if (rc) {
+    mlb_state_free(s);
+    return fail(rc, "init kernel");
+  }
+  *out = s;
+  return MLB_OK;
+}
+
+void mlb_state_free(mlb_state_t* s) {
+  if (!s) return;
+  DeviceGuard dg(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->amp) cudaFree(s->amp);
+  if (s->d_scratch) cudaFree(s->d_scratch);
+  if (s->d_plan) cudaFree(s->d_plan);
+  if (s->h_plan) cudaFreeHost(s->h_plan);
+  if (s->plan_ev) cudaEventDestroy(s->plan_ev);
+  if (s->t0) cudaEventDestroy(s->t0);
+  if (s->t1) cudaEventDestroy(s->t1);
+  if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+int mlb_state_num_qubits(const mlb_state_t* s, uint32_t* out) {
+  if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  *out = s->n;
+  return MLB_OK;
+}
+int mlb_state_dim(const mlb_state_t* s, uint64_t* out) {
+  if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  *out = 1ull << s->n;
+  return MLB_OK;
+}
+int mlb_state_dtype(const mlb_state_t* s, int* out) {
+  if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  *out = s->dtype;
+  return MLB_OK;
+}
+int mlb_state_device_ptr(mlb_state_t* s, void** out) {
+  if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  *out = s->amp;
+  return MLB_OK;
+}
+int mlb_state_set_stream(mlb_state_t* s, void* stream) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  rc = sync_stream(s);
+  if (rc) return rc;
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  if (stream) {
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+  } else {
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "stream creation");
+    s->own_stream = true;
+  }
+  return MLB_OK;
+}
+int mlb_state_stream(const mlb_state_t* s, void** out) {
+  if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  *out = (void*)s->stream;
+  return MLB_OK;
+}
+int mlb_state_set_exec_mode(mlb_state_t* s, int mode) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  if (mode != MLB_EXEC_TILED && mode != MLB_EXEC_EAGER)
+    return fail(MLB_ERR_NOT_SUPPORTED, "exec mode %d not available", mode);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  s->mode = mode;
+  return MLB_OK;
+}
+int mlb_state_reset(mlb_state_t* s) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  DeviceGuard dg(s->device);
+  s->queue.clear();
+  return launch_init_zero(s->dtype, s->amp, (int)s->n, s->stream);
+}
+int mlb_state_copy_to_host(mlb_state_t* s, void* host) {
+  if (!s || !host) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  cudaError_t e = cudaMemcpyAsync(host, s->amp, s->bytes, cudaMemcpyDeviceToHost, s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "copy to host");
+  return sync_stream(s);
+}
+int mlb_state_copy_from_host(mlb_state_t* s, const void* host) {
+  if (!s || !host) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  DeviceGuard dg(s->device);
+  s->queue.clear();  // the upload overwrites whatever was pending
+  cudaError_t e = cudaMemcpyAsync(s->amp, host, s->bytes, cudaMemcpyHostToDevice, s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "copy from host");
+  return sync_stream(s);
+}
+int mlb_state_copy(mlb_state_t* dst, mlb_state_t* src) {
+  if (!dst || !src) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (dst->n != src->n) return fail(MLB_ERR_INVALID_ARG, "qubit counts differ");
+  int rc = flush_impl(src);
+  if (rc) return rc;
+  dst->queue.clear();
+  DeviceGuard dg(dst->device);
+  rc = sync_stream(src);
+  if (rc) return rc;
+  if (dst->dtype == src->dtype) {
+    cudaError_t e = cudaMemcpyAsync(dst->amp, src->amp, src->bytes, cudaMemcpyDeviceToDevice, dst->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "state copy");
+  } else {
+    rc = launch_convert(dst->dtype, dst->amp, src->dtype, src->amp, 1ull << src->n, dst->stream);
+    if (rc) return fail(rc, "convert kernel");
+  }
+  return sync_stream(dst);
+}
+int mlb_flush(mlb_state_t* s) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  return flush_impl(s);
+}
+int mlb_synchronize(mlb_state_t* s) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  DeviceGuard dg(s->device);
+  return sync_stream(s);
+}
+
+// ---- gates ----------------------------------------------------------------
+int mlb_apply_op(mlb_state_t* s, const mlb_op_t* op) {
+  if (!s || !op) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  return enqueue(s, *op);
+}
+int mlb_apply_ops(mlb_state_t* s, const mlb_op_t* ops, size_t num) {
+  if (!s || (!ops && num)) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  for (size_t i = 0; i < num; i++) {
+    int rc = enqueue(s, ops[i]);
+    if (rc) return rc;
+  }
+  return MLB_OK;
+}
+int mlb_apply_1q(mlb_state_t* s, uint32_t t, const double m[8]) {
+  if (!m) return fail(MLB_ERR_INVALID_ARG, "null matrix");
+  mlb_op_t o{};
+  o.kind = MLB_OP_1Q;
+  o.target = (int)t;
+  o.target2 = -1;
+  std::memcpy(o.m, m, 8 * sizeof(double));
+  return enqueue(s, o);
+}
+int mlb_apply_2q(mlb_state_t* s, uint32_t q0, uint32_t q1, const double m[32]) {
+  if (!m) return fail(MLB_ERR_INVALID_ARG, "null matrix");
+  mlb_op_t o{};
+  o.kind = MLB_OP_2Q;
+  o.target = (int)q0;
+  o.target2 = (int)q1;
+  std::memcpy(o.m, m, 32 * sizeof(double));
+  return enqueue(s, o);
+}
+int mlb_apply_controlled_1q(mlb_state_t* s, uint64_t cmask, uint32_t t, const double m[8]) {
+  if (!m) return fail(MLB_ERR_INVALID_ARG, "null matrix");
+  mlb_op_t o{};
+  o.kind = MLB_OP_1Q;
+  o.target = (int)t;
+  o.target2 = -1;
+  o.cmask = cmask;
+  std::memcpy(o.m, m, 8 * sizeof(double));
+  return enqueue(s, o);
+}
+int mlb_apply_mcx(mlb_state_t* s, uint64_t cmask, uint32_t t) {
+  mlb_op_t o{};
+  o.kind = MLB_OP_X;
+  o.target = (int)t;
+  o.target2 = -1;
+  o.cmask = cmask;
+  return enqueue(s, o);
+}
+int mlb_apply_mcz(mlb_state_t* s, uint64_t all_mask) {
+  mlb_op_t o{};
+  o.kind = MLB_OP_PHASE;
+  o.target = all_mask ? __builtin_ctzll(all_mask) : 0;
+  o.target2 = -1;
+  o.cmask = all_mask;
+  o.m[0] = -1.0;
+  o.m[1] = 0.0;
+  return enqueue(s, o);
+}
+int mlb_apply_swap(mlb_state_t* s, uint64_t cmask, uint32_t q0, uint32_t q1) {
+  mlb_op_t o{};
+  o.kind = MLB_OP_SWAP;
+  o.target = (int)q0;
+  o.target2 = (int)q1;
+  o.cmask = cmask;
+  return enqueue(s, o);
+}
+int mlb_apply_zz(mlb_state_t* s, uint32_t q0, uint32_t q1, double theta) {
+  mlb_op_t o{};
+  o.kind = MLB_OP_ZZ;
+  o.target = (int)q0;
+  o.target2 = (int)q1;
+  mlb_mat_zz(theta, o.m);
+  return enqueue(s, o);
+}
+
+// ---- reductions -----------------------------------------------------------
+static int probs_z(mlb_state_t* s, std::vector<double>& out) {
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  const uint64_t dim = 1ull << s->n;
+  const uint64_t chunks = s->n >= 13 ? dim >> 13 : 1;
+  const size_t need = sizeof(double) * ((size_t)s->num_sms * 4 * 14 + chunks + 64 + 64);
+  rc = ensure_scratch(s, need);
+  if (rc) return rc;
+  double* d_out = s->d_scratch;
+  rc = launch_reduce_probs_z(s->dtype, s->amp, (int)s->n, d_out, s->d_scratch + 64, s->num_sms, s->stream);
+  if (rc) return fail(rc, "reduction launch");
+  out.assign(s->n + 1, 0.0);
+  cudaError_t e = cudaMemcpyAsync(out.data(), d_out, (s->n + 1) * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "reduction readback");
+  return sync_stream(s);
+}
+
+int mlb_norm_sq(mlb_state_t* s, double* out) {
+  if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  std::vector<double> v;
+  int rc = probs_z(s, v);
+  if (rc) return rc;
+  *out = v[s->n];
+  return MLB_OK;
+}
+int mlb_prob_one_all(mlb_state_t* s, double* out_n) {
+  if (!s || !out_n) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  std::vector<double> v;
+  int rc = probs_z(s, v);
+  if (rc) return rc;
+  std::memcpy(out_n, v.data(), s->n * sizeof(double));
+  return MLB_OK;
+}
+int mlb_prob_one(mlb_state_t* s, uint32_t q, double* out) {
+  if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (q >= s->n) return fail(MLB_ERR_INVALID_QUBIT, "qubit %u", q);
+  std::vector<double> v;
+  int rc = probs_z(s, v);
+  if (rc) return rc;
+  *out = v[q];
+  return MLB_OK;
+}
+static int seq_sum(mlb_state_t* s, uint64_t fmask, uint64_t fval, bool fused, double* total);
+
+int mlb_prob_one_exact(mlb_state_t* s, uint32_t q, double* out) {
+  if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (q >= s->n) return fail(MLB_ERR_INVALID_QUBIT, "qubit %u", q);
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  return seq_sum(s, 1ull << q, 1ull << q, true, out);
+}
+int mlb_expect_z_all(mlb_state_t* s, double* out_n) {
+  int rc = mlb_prob_one_all(s, out_n);
+  if (rc) return rc;
+  for (uint32_t q = 0; q < s->n; q++) out_n[q] = 1.0 - 2.0 * out_n[q];
+  return MLB_OK;
+}
+
+int mlb_expect_pauli_sum(mlb_state_t* s, size_t num_terms, const uint64_t* xm, const uint64_t* zm,
+                         const double* coeffs, double* out) {
+  if (!s || !out || (num_terms && (!xm || !zm))) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  const uint64_t allm = s->n >= 64 ? ~0ull : ((1ull << s->n) - 1ull);
+  for (size_t t = 0; t < num_terms; t++)
+    if ((xm[t] | zm[t]) & ~allm) return fail(MLB_ERR_INVALID_QUBIT, "Pauli term %zu outside the register", t);
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  // group terms by X mask (<= 16 per launch)
+  std::vector<size_t> order(num_terms);
+  for (size_t i = 0; i < num_terms; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return xm[a] < xm[b]; });
+  const size_t need = sizeof(double) * ((size_t)s->num_sms * 8 * 16 + 64) + 64 * (sizeof(uint64_t) + sizeof(int)) + 256;
+  rc = ensure_scratch(s, need);
+  if (rc) return rc;
+  std::vector<double> vals(num_terms, 0.0);
+  double* d_terms = s->d_scratch;
+  uint64_t* d_z = reinterpret_cast<uint64_t*>(s->d_scratch + 16);
+  int* d_ny = reinterpret_cast<int*>(s->d_scratch + 32);
+  double* d_parts = s->d_scratch + 64;
+  size_t i = 0;
+  while (i < num_terms) {
+    const uint64_t x = xm[order[i]];
+    size_t j = i;
+    uint64_t hz[16];
+    int hny[16];
+    while (j < num_terms && xm[order[j]] == x && j - i < 16) {
+      hz[j - i] = zm[order[j]];
+      hny[j - i] = popc(xm[order[j]] & zm[order[j]]);
+      j++;
+    }
+    const int cnt = (int)(j - i);
+    cudaMemcpyAsync(d_z, hz, cnt * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream);
+    cudaMemcpyAsync(d_ny, hny, cnt * sizeof(int), cudaMemcpyHostToDevice, s->stream);
+    rc = launch_pauli_group(s->dtype, s->amp, (int)s->n, x, cnt, d_z, d_ny, d_terms, d_parts, s->num_sms, s->stream);
+    if (rc) return fail(rc, "pauli launch");
+    double hv[16];
+    cudaMemcpyAsync(hv, d_terms, cnt * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    rc = sync_stream(s);
+    if (rc) return rc;
+    for (int k = 0; k < cnt; k++) vals[order[i + k]] = hv[k];
+    i = j;
+  }
+  double acc = 0.0;
+  for (size_t t = 0; t < num_terms; t++) acc += (coeffs ? coeffs[t] : 1.0) * vals[t];
+  *out = acc;
+  return MLB_OK;
+}
+int mlb_expect_pauli(mlb_state_t* s, uint64_t xmask, uint64_t zmask, double* out) {
+  const double one = 1.0;
+  return mlb_expect_pauli_sum(s, 1, &xmask, &zmask, &one, out);
+}
+int mlb_correlation_zz(mlb_state_t* s, uint32_t q1, uint32_t q2, double* out) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  if (q1 >= s->n || q2 >= s->n) return fail(MLB_ERR_INVALID_QUBIT, "qubit out of range");
+  const uint64_t z = (1ull << q1) ^ (1ull << q2);
+  return mlb_expect_pauli(s, 0, z, out);
+}
+
+int mlb_probabilities(mlb_state_t* s, int rule, double* out_host, void* out_device) {
+  if (!s || (!out_host && !out_device)) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (rule != 0 && rule != 1) return fail(MLB_ERR_INVALID_ARG, "rule %d", rule);
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  const uint64_t dim = 1ull << s->n;
+  double* dst = (double*)out_device;
+  bool temp = false;
+  if (!dst) {
+    cudaError_t e = cudaMallocAsync((void**)&dst, dim * sizeof(double), s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "probability buffer");
+    temp = true;
+  }
+  rc = launch_probabilities(s->dtype, s->amp, (int)s->n, rule, dst, s->stream);
+  if (rc) return fail(rc, "probability kernel");
+  if (out_host) {
+    cudaError_t e = cudaMemcpyAsync(out_host, dst, dim * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "probability readback");
+  }
+  if (temp) cudaFreeAsync(dst, s->stream);
+  return sync_stream(s);
+}
+
+// ---- sampling / collapse ---------------------------------------------------
+int mlb_sample(mlb_state_t* s, int rule, const double* u, size_t num, uint64_t* out) {
+  if (!s || (num && (!u || !out))) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (rule != MLB_SAMPLE_CDF_GE && rule != MLB_SAMPLE_CUM_GT) return fail(MLB_ERR_INVALID_ARG, "rule %d", rule);
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  char eb[8];
+  rc = sample_exact(s->dtype, s->amp, (int)s->n, rule, u, num, out, s->num_sms, s->stream, eb, sizeof eb);
+  if (rc) return fail(rc, "sampling: %s", cudaGetErrorString(cudaGetLastError()));
+  return MLB_OK;
+}
+
+static int seq_sum(mlb_state_t* s, uint64_t fmask, uint64_t fval, bool fused, double* total) {
+  int rc = seq_sum_exact(s->dtype, s->amp, (int)s->n, fmask, fval, fused, s->num_sms, s->stream, total);
+  if (rc) return fail(rc, "sequential sum: %s", cudaGetErrorString(cudaGetLastError()));
+  return MLB_OK;
+}
+
+int mlb_measure_qubit(mlb_state_t* s, uint32_t q, double u, int* outcome) {
+  if (!s || !outcome) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (q >= s->n) return fail(MLB_ERR_INVALID_QUBIT, "qubit %u", q);
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  const uint64_t b = 1ull << q;
+  // measurement_probability_one and the kept-half norm both accumulate with
+  // fused multiply-adds in the reference build (measurement.c:93, :214).
+  double p1 = 0.0;
+  rc = seq_sum(s, b, b, true, &p1);
+  if (rc) return rc;
+  const int r = (u < p1) ? 1 : 0;
+  double nf = p1;
+  if (r == 0) {
+    rc = seq_sum(s, b, 0, true, &nf);
+    if (rc) return rc;
+  }
+  if (nf <= 1e-15) {  // zero the other half, leave unnormalised (measurement.c:222-231)
+    rc = launch_scale(s->dtype, s->amp, (int)s->n, 1.0, b, r ? b : 0, s->stream);
+    if (rc) return fail(rc, "collapse kernel");
+    *outcome = -1;
+    return sync_stream(s);
+  }
+  const double inv = 1.0 / std::sqrt(nf);
+  rc = launch_scale(s->dtype, s->amp, (int)s->n, inv, b, r ? b : 0, s->stream);
+  if (rc) return fail(rc, "collapse kernel");
+  *outcome = r;
+  return sync_stream(s);
+}
+
+int mlb_quantum_measure(mlb_state_t* s, uint32_t q, double u, int* outcome, double* probability) {
+  if (!s || !outcome) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (q >= s->n) return fail(MLB_ERR_INVALID_QUBIT, "qubit %u", q);
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  const uint64_t b = 1ull << q;
+  double p0 = 0.0, p1 = 0.0;
+  // quantum_measure rounds product and sum separately (gates.c:1150-1199).
+  if ((rc = seq_sum(s, b, 0, false, &p0))) return rc;
+  if ((rc = seq_sum(s, b, b, false, &p1))) return rc;
+  const int r = (u < p0) ? 0 : 1;
+  const double keep = r == 0 ? p0 : p1;
+  if (probability) *probability = keep;
+  if (keep <= 1e-15) {  // gates.c:1203-1205: dropped half zeroed, result {0, 0}
+    rc = launch_scale(s->dtype, s->amp, (int)s->n, 1.0, b, r ? b : 0, s->stream);
+    if (rc) return fail(rc, "collapse kernel");
+    *outcome = 0;
+    if (probability) *probability = 0.0;
+    return sync_stream(s);
+  }
+  const double nrm = std::sqrt(keep);
+  rc = launch_scale(s->dtype, s->amp, (int)s->n, -nrm, b, r ? b : 0, s->stream);  // divide
+  if (rc) return fail(rc, "collapse kernel");
+  *outcome = r;
+  return sync_stream(s);
+}
+
+int mlb_measure_all(mlb_state_t* s, double u, uint64_t* outcome) {
+  if (!s || !outcome) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  int rc = mlb_sample(s, MLB_SAMPLE_CUM_GT, &u, 1, outcome);
+  if (rc) return rc;
+  DeviceGuard dg(s->device);
+  // collapse to |outcome>: zero everything, then write 1 at the index
+  cudaError_t e = cudaMemsetAsync(s->amp, 0, s->bytes, s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "collapse memset");
+  if (s->dtype == MLB_C128) {
+    const double one[2] = {1.0, 0.0};
+    e = cudaMemcpyAsync((char*)s->amp + 16 * (*outcome), one, 16, cudaMemcpyHostToDevice, s->stream);
+  } else {
+    const float one[2] = {1.0f, 0.0f};
+    e = cudaMemcpyAsync((char*)s->amp + 8 * (*outcome), one, 8, cudaMemcpyHostToDevice, s->stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "collapse write");
+  return sync_stream(s);
+}
+
+int mlb_normalize(mlb_state_t* s, double* norm_out) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  double nsq = 0.0;
+  int rc = mlb_norm_sq(s, &nsq);
+  if (rc) return rc;
+  const double nrm = std::sqrt(nsq);
+  if (norm_out) *norm_out = nrm;
+  if (nrm < 1e-15) return fail(MLB_ERR_INVALID_ARG, "state norm %g too small to normalise", nrm);
+  DeviceGuard dg(s->device);
+  rc = launch_scale(s->dtype, s->amp, (int)s->n, -nrm, 0, 0, s->stream);
+  if (rc) return fail(rc, "normalise kernel");
+  return sync_stream(s);
+}
+
+// ---- circuits -------------------------------------------------------------
+int mlb_gates_to_ops(const mlb_gate_t* gates, size_t num, uint32_t n, mlb_op_t* ops, size_t* num_ops) {
+  if ((!gates && num) || !num_ops) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  size_t k = 0;
+  auto emit = [&](const mlb_op_t& o) {
+    if (ops) ops[k] = o;
+    k++;
+  };
+  auto one = [&](int t, const double m[8]) {
+    mlb_op_t o{};
+    o.kind = MLB_OP_1Q;
+    o.target = t;
+    o.target2 = -1;
+    std::memcpy(o.m, m, 8 * sizeof(double));
+    emit(o);
+  };
+  for (size_t i = 0; i < num; i++) {
+    const mlb_gate_t& g = gates[i];
+    const int t = g.target, c = g.control;
+    auto qok = [&](int q) { return q >= 0 && (uint32_t)q < n; };
+    if (g.type != 0 && !qok(t)) return fail(MLB_ERR_INVALID_QUBIT, "gate %zu: target %d", i, t);
+    const bool two = (g.type >= 10 && g.type <= 13) || (g.type >= 23 && g.type <= 26);
+    if ((two || g.type == MLB_GATE_ZZ) && (!qok(c) || c == t))
+      return fail(MLB_ERR_INVALID_QUBIT, "gate %zu: qubits (%d,%d)", i, c, t);
+    double m[8];
+    switch (g.type) {
+      case 0: break;                                               // I
+      case 1: { mlb_op_t o{}; o.kind = MLB_OP_X; o.target = t; o.target2 = -1; emit(o); break; }
+      case 2: { const double y[8] = {0, 0, 0, -1, 0, 1, 0, 0}; one(t, y); break; }   // gates.c:162
+      case 3: { const double z[8] = {1, 0, 0, 0, 0, 0, -1, 0}; one(t, z); break; }   // gates.c:203
+      case 4: {                                                                       // H
+        const double r = 0.70710678118654752440;
+        const double h[8] = {r, 0, r, 0, r, 0, -r, 0};
+        one(t, h);
+        break;
+      }
+      case 5: { const double sm[8] = {1, 0, 0, 0, 0, 0, 0, 1}; one(t, sm); break; }  // S
+      case 6: mlb_mat_phase1(0, 0.0, m); one(t, m); break;                            // T
+      case 7: mlb_mat_rx(g.theta, m); one(t, m); break;
+      case 8: mlb_mat_ry(g.theta, m); one(t, m); break;
+      case 9: mlb_mat_rz(g.theta, m); one(t, m); break;
+      case 10: { mlb_op_t o{}; o.kind = MLB_OP_X; o.target = t; o.target2 = -1; o.cmask = 1ull << c; emit(o); break; }
+      case 11: {  // CY composed as S . CNOT . Sdg (moonlab_qgtl_backend.c:138-144)
+        const double sm[8] = {1, 0, 0, 0, 0, 0, 0, 1}, sd[8] = {1, 0, 0, 0, 0, 0, 0, -1};
+        one(t, sm);
+        mlb_op_t o{}; o.kind = MLB_OP_X; o.target = t; o.target2 = -1; o.cmask = 1ull << c; emit(o);
+        one(t, sd);
+        break;
+      }
+      case 12: { mlb_op_t o{}; o.kind = MLB_OP_PHASE; o.target = t; o.target2 = c; o.cmask = (1ull << t) | (1ull << c); o.m[0] = -1.0; emit(o); break; }
+      case 13: { mlb_op_t o{}; o.kind = MLB_OP_SWAP; o.target = c; o.target2 = t; emit(o); break; }
+      case MLB_GATE_ZZ: { mlb_op_t o{}; o.kind = MLB_OP_ZZ; o.target = c; o.target2 = t; mlb_mat_zz(g.theta, o.m); emit(o); break; }
+      case 20: { const double sd[8] = {1, 0, 0, 0, 0, 0, 0, -1}; one(t, sd); break; }  // Sdg, gates.c:352
+      case 21: mlb_mat_phase1(1, 0.0, m); one(t, m); break;                            // Tdg
+      case 22: mlb_mat_phase1(2, g.theta, m); one(t, m); break;                        // phase(theta)
+      case 23: {  // CPHASE: diag(1,1,1,e^{i theta}) (gates.c:743-754)
+        mlb_op_t o{}; o.kind = MLB_OP_PHASE; o.target = t; o.target2 = c;
+        o.cmask = (1ull << t) | (1ull << c); mlb_mat_cphase(g.theta, o.m); emit(o); break;
+      }
+      case 24: case 25: case 26: {  // CRX / CRY / CRZ GPU routes (gates.c:800-887)
+        if (g.type == 24) mlb_mat_rx(g.theta, m);
+        else if (g.type == 25) mlb_mat_ry(g.theta, m);
+        else mlb_mat_crz_inner(g.theta, m);
+        mlb_op_t o{}; o.kind = MLB_OP_1Q; o.target = t; o.target2 = -1; o.cmask = 1ull << c;
+        std::memcpy(o.m, m, sizeof m); emit(o); break;
+      }
+      default: return fail(MLB_ERR_NOT_SUPPORTED, "gate %zu: type %d", i, g.type);
+    }
+  }
+  *num_ops = k;
+  return MLB_OK;
+}
+
+int mlb_run_gates(mlb_state_t* s, const mlb_gate_t* gates, size_t num) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  size_t cnt = 0;
+  int rc = mlb_gates_to_ops(gates, num, s->n, nullptr, &cnt);
+  if (rc) return rc;
+  std::vector<mlb_op_t> ops(cnt);
+  rc = mlb_gates_to_ops(gates, num, s->n, ops.data(), &cnt);
+  if (rc) return rc;
+  return mlb_apply_ops(s, ops.data(), cnt);
+}
+
+int mlb_plan_ops(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fuse1q,
+                 mlb_flush_stats_t* out) {
+  if ((!ops && num) || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (n < 1 || n > 34 || (dtype != MLB_C128 && dtype != MLB_C64)) return fail(MLB_ERR_INVALID_ARG, "bad shape");
+  mlb_state probe;  // host-side only: validation needs n
+  probe.n = n;
+  std::vector<mlb_op_t> q;
+  q.reserve(num);
+  for (size_t i = 0; i < num; i++) {
+    int rc = validate(&probe, ops[i]);
+    if (rc) return rc;
+    q.push_back(canonical(ops[i]));
+  }
+  std::vector<mlb_op_t> fused = fuse1q ? fuse_1q_runs(q, n) : q;
+  Planner pl{n, dtype, geo(dtype), {}, {}, {}};
+  pl.plan(fused);
+  mlb_flush_stats_t st{};
+  st.passes = pl.passes.size();
+  st.ops = fused.size();
+  st.kernel_launches = pl.passes.size();
+  st.bytes_moved = st.passes * 2ull * (dtype == MLB_C128 ? 16ull : 8ull) * (1ull << n);
+  *out = st;
+  return MLB_OK;
+}
+
+int mlb_last_flush_stats(mlb_state_t* s, mlb_flush_stats_t* out) {
+  if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (s->timed_pending) {
+    DeviceGuard dg(s->device);
+    cudaError_t e = cudaEventSynchronize(s->t1);
+    if (e != cudaSuccess) return cuda_fail(e, "timing event");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s->t0, s->t1);
+    s->stats.gpu_ms = ms;
+    s->timed_pending = false;
+  }
+  *out = s->stats;
+  return MLB_OK;
+}
+int mlb_state_set_timing(mlb_state_t* s, int enable) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  DeviceGuard dg(s->device);
+  if (enable && !s->t0) {
+    cudaError_t e = cudaEventCreate(&s->t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->t1);
+    if (e != cudaSuccess) return cuda_fail(e, "timing events");
+  }
+  s->timing = enable != 0;
+  return MLB_OK;
+}
+int mlb_total_kernel_launches(uint64_t* out) {
+  if (!out) return fail(MLB_ERR_INVALID_ARG, "null argument");
+  *out = kernel_launch_count();
+  return MLB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,519 @@
+// kernels_sample.cu -- the reference's sequential FP64 sums, reproduced
+// exactly on the GPU, and sampling / collapse built on them.
+//
+// The reference draws outcomes from a left-to-right running sum
+//     s_i = fl(s_{i-1} + p_i),  p_i = fl(cabs(a_i) * cabs(a_i))
+// (measurement_sample, measurement.c:551-601; measurement_all_qubits,
+// :263-307; qgtl shots, moonlab_qgtl_backend.c:218-243) and decides
+// single-qubit outcomes from the same kind of sum over half of the indices
+// (measurement_probability_one, measurement.c:73; quantum_measure,
+// gates.c:1117-1241).  A parallel sum rounds differently, so an outcome
+// near a CDF boundary could differ.  This file reproduces s_i exactly:
+//
+//  * p_i: hypot_glibc.cuh reproduces glibc's cabs bit for bit.
+//  * Within one binade [2^e, 2^(e+1)) every representable s is a multiple of
+//    g = ulp(2^e), so fl(s + p) = s + g * k with k = p/g rounded to nearest,
+//    ties to the k that makes (s/g + k) even.  Only the tie case depends on
+//    s, and only through the parity of s/g.  A chunk of elements therefore
+//    maps (N = s/g, parity) -> (N + K[parity], parity') with two integer
+//    increments, computed in parallel as an ordered reduction of 2-entry
+//    transfer tables (phase C).  Chunks are chained serially from the exact
+//    running value (phase D); a chunk whose sum leaves the binade, whose
+//    predicted binade was wrong, or which starts at s = 0 is summed element
+//    by element instead.  The binade of each chunk's start is predicted from
+//    an ordinary parallel prefix of chunk totals (phases A, B).
+//  * Sampling (phase E): one warp per uniform finds the chunk whose exact
+//    end value first passes u and replays that chunk's adds in hardware
+//    FP64 (IEEE round to nearest, hence bit-identical).
+//
+// A filter (index & fmask) == fval restricts the sum to a subspace: elements
+// outside it contribute p = 0, and fl(s + 0) = s, so the filtered running
+// sum equals the reference's sum over the subspace in index order.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "hypot_glibc.cuh"
+#include "kernels_common.cuh"
+#include "mlb_internal.h"
+
+namespace mlb {
+
+namespace {
+
+constexpr int kCB = 12;             // chunk = 2^12 elements (33 KiB of p in shared memory)
+constexpr int kCT = 256;            // threads per CTA
+constexpr int kPer = (1 << kCB) / kCT;  // 32 contiguous elements per thread
+constexpr long long kTwo53 = 1ll << 53;
+
+struct Xfer {          // per chunk: transfer tables for two candidate binades
+  int32_t e[2];        // binade exponents (INT32_MIN: unused)
+  long long K[2][2];   // [candidate][entry parity] increments, saturated at 2^53
+  int32_t P[2][2];     // exit parity
+};
+
+struct SeqScratch {
+  double* chunk_tot;   // [nc] plain FP64 chunk totals (phase A)
+  double* chunk_pre;   // [nc] exclusive prefix of chunk totals (phase B)
+  Xfer* xfer;          // [nc]
+  double* s_in;        // [nc + 1] exact running value before chunk c; s_in[nc] = total
+  long long* lastnz;   // [1] largest index with p > 0 (within the filter), -1 if none
+  double* uni;         // [num] uniforms (sampling)
+  unsigned long long* outc;  // [num] outcomes (sampling)
+};
+
+template <typename Real>
+__device__ __forceinline__ double elem_p(const typename Cplx<Real>::T* __restrict__ amp, uint64_t i,
+                                         uint64_t fmask, uint64_t fval) {
+  if ((i & fmask) != fval) return 0.0;
+  const auto a = amp[i];
+  return glibc_prob((double)a.x, (double)a.y);
+}
+
+// Two accumulation contracts, as the reference's Release build compiles its
+// loops: SEPARATE  s = fl(s + fl(h*h))   (measurement_sample,
+// measurement_all_qubits, quantum_measure) and FUSED  s = fma(h, h, s)
+// (measurement_probability_one, measurement_single_qubit).  The per-element
+// value kept in shared memory is p = fl(h*h) for SEPARATE and h for FUSED.
+template <typename Real, bool FUSED>
+__device__ __forceinline__ double elem_val(const typename Cplx<Real>::T* __restrict__ amp, uint64_t i,
+                                           uint64_t fmask, uint64_t fval) {
+  if ((i & fmask) != fval) return 0.0;
+  const auto a = amp[i];
+  const double h = glibc_cabs((double)a.x, (double)a.y);
+  return FUSED ? h : __dmul_rn(h, h);
+}
+template <bool FUSED>
+__device__ __forceinline__ double elem_add(double s, double v) {
+  return FUSED ? __fma_rn(v, v, s) : __dadd_rn(s, v);
+}
+template <bool FUSED>
+__device__ __forceinline__ double elem_approx(double v) {
+  return FUSED ? v * v : v;
+}
+
+// binade exponent of s > 0 (s in [2^e, 2^(e+1))) and its grid spacing
+__device__ __forceinline__ int binade_of(double s) {
+  const unsigned long long b = __double_as_longlong(s);
+  const int ex = (int)((b >> 52) & 0x7ff);
+  if (ex == 0) return -1023;  // subnormal: grid 2^-1074
+  return ex - 1023;
+}
+__device__ __forceinline__ double grid_of(int e) {
+  const int ge = e - 52;
+  return ge < -1074 ? 0x1p-1074 : ldexp(1.0, ge);
+}
+
+// Load a chunk's p values into shared memory (coalesced) -- p[j] for j in
+// [0, len), padded by one slot per 32 to spread banks for the contiguous
+// per-thread reads that follow.
+template <typename Real, bool FUSED>
+__device__ __forceinline__ void load_chunk_p(const typename Cplx<Real>::T* __restrict__ amp,
+                                             uint64_t base, uint32_t len, uint64_t fmask,
+                                             uint64_t fval, double* sp) {
+  for (uint32_t j = threadIdx.x; j < len; j += kCT)
+    sp[j + (j >> 5)] = elem_val<Real, FUSED>(amp, base + j, fmask, fval);
+}
+
+// Phase A: chunk totals (plain FP64, ordered) and the last nonzero index.
+template <typename Real, bool FUSED>
+__global__ void __launch_bounds__(kCT) k_seq_a(const typename Cplx<Real>::T* __restrict__ amp,
+                                               uint64_t nc, uint32_t clen, uint64_t fmask,
+                                               uint64_t fval, double* __restrict__ chunk_tot,
+                                               long long* __restrict__ lastnz) {
+  __shared__ double sp[(1 << kCB) + (1 << kCB) / 32];
+  __shared__ double red[kCT / 32];
+  __shared__ long long redl[kCT / 32];
+  for (uint64_t c = blockIdx.x; c < nc; c += gridDim.x) {
+    const uint64_t base = c * clen;
+    load_chunk_p<Real, FUSED>(amp, base, clen, fmask, fval, sp);
+    __syncthreads();
+    double t = 0.0;
+    long long lnz = -1;
+    for (int k = 0; k < kPer; k++) {
+      const uint32_t j = threadIdx.x * kPer + k;
+      if (j < clen) {
+        const double p = elem_approx<FUSED>(sp[j + (j >> 5)]);
+        t += p;
+        if (p > 0.0) lnz = (long long)(base + j);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      t += __shfl_down_sync(0xffffffffu, t, o);
+      lnz = max(lnz, __shfl_down_sync(0xffffffffu, lnz, o));
+    }
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = t; redl[threadIdx.x >> 5] = lnz; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tt = 0.0;
+      long long ll = -1;
+      for (int w = 0; w < kCT / 32; w++) { tt += red[w]; ll = max(ll, redl[w]); }
+      chunk_tot[c] = tt;
+      if (ll >= 0) atomicMax(lastnz, ll);
+    }
+    __syncthreads();
+  }
+}
+
+// Phase B: exclusive prefix of chunk totals (one CTA; fixed order).
+__global__ void __launch_bounds__(1024) k_seq_b(const double* __restrict__ tot, uint64_t nc,
+                                                double* __restrict__ pre) {
+  __shared__ double part[1024];
+  const uint64_t per = (nc + 1023) / 1024;
+  const uint64_t lo = threadIdx.x * per, hi = min(nc, lo + per);
+  double s = 0.0;
+  for (uint64_t c = lo; c < hi; c++) s += tot[c];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double run = 0.0;
+    for (int i = 0; i < 1024; i++) { const double v = part[i]; part[i] = run; run += v; }
+  }
+  __syncthreads();
+  double run = part[threadIdx.x];
+  for (uint64_t c = lo; c < hi; c++) { pre[c] = run; run += tot[c]; }
+}
+
+struct Fn {  // transfer table: entry parity -> (increment, exit parity)
+  long long K0, K1;
+  int P0, P1;
+};
+__device__ __forceinline__ long long sat_add(long long a, long long b) {
+  const long long r = a + b;
+  return r > kTwo53 ? kTwo53 : r;
+}
+__device__ __forceinline__ Fn compose(const Fn& f, const Fn& g) {  // g after f
+  Fn r;
+  r.K0 = sat_add(f.K0, f.P0 ? g.K1 : g.K0);
+  r.P0 = f.P0 ? g.P1 : g.P0;
+  r.K1 = sat_add(f.K1, f.P1 ? g.K1 : g.K0);
+  r.P1 = f.P1 ? g.P1 : g.P0;
+  return r;
+}
+
+// Element transfer on grid g (inv_g = 1/g, an exact power of two).  The
+// element adds the exact real v = hi + lo to the running sum: SEPARATE has
+// v = p (lo = 0); FUSED has v = h*h exactly, hi = fl(h*h), lo = fma(h,h,-hi).
+// With q = v/g = qh + ql (both exact scalings), fl = floor(qh) and
+// r = qh - fl (exact), the nearest integer to q is fl + 1 when r > 1/2 or
+// (r == 1/2 and ql > 0), fl when r < 1/2 or (r == 1/2 and ql < 0), and a tie
+// only when r == 1/2 and ql == 0: |ql| <= ulp(qh)/2 and r lies on qh's
+// grid, so ql can only decide the case r == 1/2.
+template <bool FUSED>
+__device__ __forceinline__ Fn elem_fn(double v, double inv_g) {
+  Fn f;
+  if (v == 0.0) { f.K0 = 0; f.K1 = 0; f.P0 = 0; f.P1 = 1; return f; }
+  double hi = v, lo = 0.0;
+  if (FUSED) {
+    hi = __dmul_rn(v, v);
+    lo = __fma_rn(v, v, -hi);
+    if (hi == 0.0) { f.K0 = 0; f.K1 = 0; f.P0 = 0; f.P1 = 1; return f; }
+  }
+  const double q = hi * inv_g;  // exact scaling by a power of two
+  if (!(q < 0x1p53)) { f.K0 = kTwo53; f.K1 = kTwo53; f.P0 = 0; f.P1 = 0; return f; }
+  const double ql = lo * inv_g;
+  const double fl = floor(q);
+  const double fr = q - fl;   // exact
+  const long long k = (long long)fl;
+  const bool up = fr > 0.5 || (fr == 0.5 && ql > 0.0);
+  const bool down = fr < 0.5 || (fr == 0.5 && ql < 0.0);
+  if (up || down) {
+    const long long kk = k + (up ? 1 : 0);
+    f.K0 = kk; f.K1 = kk;
+    f.P0 = (int)(kk & 1);
+    f.P1 = (int)((kk + 1) & 1);
+    return f;
+  }
+  // tie: choose the increment that makes N + increment even
+  const long long k0 = k + ((0 + k) & 1);   // entry parity 0
+  const long long k1 = k + ((1 + k) & 1);   // entry parity 1
+  f.K0 = k0; f.K1 = k1; f.P0 = 0; f.P1 = 0;
+  return f;
+}
+
+// Phase C: transfer tables for the two candidate binades of each chunk.
+template <typename Real, bool FUSED>
+__global__ void __launch_bounds__(kCT) k_seq_c(const typename Cplx<Real>::T* __restrict__ amp,
+                                               uint64_t nc, uint32_t clen, uint64_t fmask,
+                                               uint64_t fval, const double* __restrict__ pre,
+                                               Xfer* __restrict__ xfer) {
+  __shared__ double sp[(1 << kCB) + (1 << kCB) / 32];
+  __shared__ Fn red[kCT / 32][2];
+  const double u = 0x1p-53;
+  for (uint64_t c = blockIdx.x; c < nc; c += gridDim.x) {
+    const uint64_t base = c * clen;
+    // candidate binades of the running value at the chunk start: the
+    // prefix estimate +- a bound on both its error and the reference's.
+    const double S = pre[c];
+    int ecand[2] = {INT32_MIN, INT32_MIN};
+    if (S > 0.0) {
+      const double rel = ((double)base * 4.0 + 1.0e6) * u;
+      const int elo = binade_of(S * (1.0 - rel)), ehi = binade_of(S * (1.0 + rel));
+      ecand[0] = elo;
+      ecand[1] = (ehi == elo) ? INT32_MIN : ehi;
+      if (ehi - elo > 1) { ecand[0] = INT32_MIN; ecand[1] = INT32_MIN; }  // too uncertain
+    }
+    load_chunk_p<Real, FUSED>(amp, base, clen, fmask, fval, sp);
+    __syncthreads();
+    Fn tot[2];
+    for (int cand = 0; cand < 2; cand++) {
+      Fn acc = {0, 0, 0, 1};  // identity
+      if (ecand[cand] != INT32_MIN) {
+        const double inv_g = 1.0 / grid_of(ecand[cand]);
+        for (int k = 0; k < kPer; k++) {
+          const uint32_t j = threadIdx.x * kPer + k;
+          if (j < clen) acc = compose(acc, elem_fn<FUSED>(sp[j + (j >> 5)], inv_g));
+        }
+      }
+      // ordered warp reduction: lane l combines [l, l+o) with [l+o, l+2o)
+      for (int o = 1; o < 32; o <<= 1) {
+        Fn other;
+        other.K0 = __shfl_down_sync(0xffffffffu, acc.K0, o);
+        other.K1 = __shfl_down_sync(0xffffffffu, acc.K1, o);
+        other.P0 = __shfl_down_sync(0xffffffffu, acc.P0, o);
+        other.P1 = __shfl_down_sync(0xffffffffu, acc.P1, o);
+        if ((threadIdx.x & 31) + o < 32 && ((threadIdx.x & (2 * o - 1)) == 0)) acc = compose(acc, other);
+      }
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][cand] = acc;
+      tot[cand] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      Xfer x;
+      for (int cand = 0; cand < 2; cand++) {
+        Fn a = {0, 0, 0, 1};
+        for (int w = 0; w < kCT / 32; w++) a = compose(a, red[w][cand]);
+        x.e[cand] = ecand[cand];
+        x.K[cand][0] = a.K0; x.K[cand][1] = a.K1;
+        x.P[cand][0] = a.P0; x.P[cand][1] = a.P1;
+      }
+      xfer[c] = x;
+    }
+    (void)tot;
+    __syncthreads();
+  }
+}
+
+// Phase D: serial chain over chunks (one CTA).  Transfer tables are staged
+// into shared memory in batches; thread 0 runs the integer fast path over a
+// batch; when a chunk cannot use it, all threads recompute that chunk's p
+// values into shared memory and thread 0 replays its adds.
+constexpr int kDBatch = 128;
+template <typename Real, bool FUSED>
+__global__ void __launch_bounds__(kCT) k_seq_d(const typename Cplx<Real>::T* __restrict__ amp,
+                                               uint64_t nc, uint32_t clen, uint64_t fmask,
+                                               uint64_t fval, const Xfer* __restrict__ xfer,
+                                               double* __restrict__ s_in) {
+  __shared__ double sp[(1 << kCB) + (1 << kCB) / 32];
+  __shared__ Xfer sx[kDBatch];
+  __shared__ uint64_t s_next;
+  __shared__ double s_run;
+  uint64_t c = 0;
+  double s = 0.0;
+  while (c < nc) {
+    const uint64_t c0 = c, c1 = min(nc, c0 + kDBatch);
+    for (uint64_t i = c0 + threadIdx.x; i < c1; i += kCT) sx[i - c0] = xfer[i];
+    __syncthreads();
+    while (true) {
+      if (threadIdx.x == 0) {
+        for (; c < c1; c++) {
+          s_in[c] = s;
+          if (!(s > 0.0)) break;
+          const int e = binade_of(s);
+          const Xfer& x = sx[c - c0];
+          const int cand = (x.e[0] == e) ? 0 : (x.e[1] == e) ? 1 : -1;
+          if (cand < 0) break;
+          const double g = grid_of(e);
+          const long long N = (long long)(s / g);
+          const long long K = x.K[cand][(int)(N & 1)];
+          if (N + K >= kTwo53) break;
+          s = (double)(N + K) * g;  // exact: N + K < 2^53
+        }
+        s_next = c;
+        s_run = s;
+      }
+      __syncthreads();
+      c = s_next;
+      s = s_run;
+      if (c >= c1) break;
+      // element-by-element replay of chunk c
+      load_chunk_p<Real, FUSED>(amp, c * clen, clen, fmask, fval, sp);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (uint32_t j = 0; j < clen; j++) s = elem_add<FUSED>(s, sp[j + (j >> 5)]);
+        s_run = s;
+      }
+      __syncthreads();
+      s = s_run;
+      c++;
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) s_in[nc] = s;
+}
+
+// Phase E: one warp per uniform.
+template <typename Real>
+__global__ void __launch_bounds__(kCT) k_seq_e(const typename Cplx<Real>::T* __restrict__ amp,
+                                               uint64_t nc, uint32_t clen, uint64_t dim, int rule,
+                                               const double* __restrict__ s_in,
+                                               const long long* __restrict__ lastnz,
+                                               const double* __restrict__ uni, uint64_t num,
+                                               unsigned long long* __restrict__ out) {
+  const uint64_t w = ((uint64_t)blockIdx.x * kCT + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= num) return;
+  const double u = uni[w];
+  // first chunk c whose end value s_in[c+1] passes u (>= for rule 0, > for rule 1)
+  uint64_t lo = 0, hi = nc;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    const double end = s_in[mid + 1];
+    const bool pass = rule == 0 ? (end >= u) : (end > u);
+    if (pass) hi = mid; else lo = mid + 1;
+  }
+  if (lo >= nc) {
+    if (lane == 0) {
+      if (rule == 0) out[w] = dim - 1;
+      else out[w] = (unsigned long long)(lastnz[0] >= 0 ? lastnz[0] : 0);
+    }
+    return;
+  }
+  const uint64_t c = lo, base = c * clen;
+  double s = s_in[c];
+  unsigned long long found = ~0ull;
+  for (uint32_t j0 = 0; j0 < clen && found == ~0ull; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const double p = j < clen ? elem_p<Real>(amp, base + j, 0, 0) : 0.0;
+    // lane 0 replays the 32 adds in order
+    for (int l = 0; l < 32; l++) {
+      const double pl = __shfl_sync(0xffffffffu, p, l);
+      if (lane == 0 && found == ~0ull && j0 + l < clen) {
+        s = __dadd_rn(s, pl);
+        const bool hit = rule == 0 ? (s >= u) : (u < s);
+        if (hit) found = base + j0 + l;
+      }
+    }
+    found = __shfl_sync(0xffffffffu, found, 0);
+  }
+  if (lane == 0) {
+    // The chunk end passes u, so the replay must hit inside it.
+    out[w] = found != ~0ull ? found : (rule == 0 ? dim - 1 : (unsigned long long)base + clen - 1);
+  }
+}
+
+struct Cache {
+  int device = -1;
+  size_t bytes = 0;
+  void* mem = nullptr;
+};
+thread_local Cache g_cache;
+
+SeqScratch get_scratch(uint64_t nc, size_t num, cudaStream_t stream) {
+  const size_t need = sizeof(double) * nc * 2 + sizeof(Xfer) * nc + sizeof(double) * (nc + 1) +
+                      sizeof(long long) + sizeof(double) * num + sizeof(uint64_t) * num + 256 * 7;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (g_cache.mem == nullptr || g_cache.bytes < need || g_cache.device != dev) {
+    if (g_cache.mem) {
+      cudaStreamSynchronize(stream);
+      cudaFree(g_cache.mem);
+    }
+    g_cache.mem = nullptr;
+    if (cudaMalloc(&g_cache.mem, need) != cudaSuccess) {
+      g_cache = Cache{};
+      return SeqScratch{};
+    }
+    g_cache.bytes = need;
+    g_cache.device = dev;
+  }
+  char* p = (char*)g_cache.mem;
+  auto take = [&](size_t b) { char* r = p; p += (b + 255) & ~(size_t)255; return (void*)r; };
+  SeqScratch s;
+  s.chunk_tot = (double*)take(sizeof(double) * nc);
+  s.chunk_pre = (double*)take(sizeof(double) * nc);
+  s.xfer = (Xfer*)take(sizeof(Xfer) * nc);
+  s.s_in = (double*)take(sizeof(double) * (nc + 1));
+  s.lastnz = (long long*)take(sizeof(long long));
+  s.uni = (double*)take(sizeof(double) * num);
+  s.outc = (unsigned long long*)take(sizeof(uint64_t) * num);
+  return s;
+}
+
+// Run phases A-D; on return s_in[0..nc] are the exact running values.
+template <typename Real, bool FUSED>
+int seq_prepare(const void* amp_v, int n, uint64_t fmask, uint64_t fval, size_t num, int num_sms,
+                cudaStream_t stream, SeqScratch& sc, uint64_t& nc, uint32_t& clen) {
+  using A = typename Cplx<Real>::T;
+  const A* amp = (const A*)amp_v;
+  const uint64_t dim = 1ull << n;
+  clen = n >= kCB ? (1u << kCB) : (uint32_t)dim;
+  nc = dim / clen;
+  sc = get_scratch(nc, num, stream);
+  if (!sc.chunk_tot) return MLB_ERR_OUT_OF_MEMORY;
+  const long long neg1 = -1;
+  cudaMemcpyAsync(sc.lastnz, &neg1, sizeof(neg1), cudaMemcpyHostToDevice, stream);
+  const int grid = (int)std::min<uint64_t>(nc, (uint64_t)num_sms * 4);
+  k_seq_a<Real, FUSED><<<grid, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.chunk_tot, sc.lastnz);
+  k_seq_b<<<1, 1024, 0, stream>>>(sc.chunk_tot, nc, sc.chunk_pre);
+  k_seq_c<Real, FUSED><<<grid, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.chunk_pre, sc.xfer);
+  k_seq_d<Real, FUSED><<<1, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.xfer, sc.s_in);
+  count_launch(4);
+  return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
+}
+
+template <typename Real>
+int sample_t(const void* amp, int n, int rule, const double* h_u, size_t num, uint64_t* h_out,
+             int num_sms, cudaStream_t stream) {
+  SeqScratch sc;
+  uint64_t nc;
+  uint32_t clen;
+  int rc = seq_prepare<Real, false>(amp, n, 0, 0, num, num_sms, stream, sc, nc, clen);
+  if (rc) return rc;
+  if (num == 0) return MLB_OK;
+  double* d_u = sc.uni;
+  unsigned long long* d_o = sc.outc;
+  cudaMemcpyAsync(d_u, h_u, num * sizeof(double), cudaMemcpyHostToDevice, stream);
+  const uint64_t threads = num * 32;
+  const unsigned grid = (unsigned)((threads + kCT - 1) / kCT);
+  k_seq_e<Real><<<grid, kCT, 0, stream>>>((const typename Cplx<Real>::T*)amp, nc, clen, 1ull << n,
+                                          rule, sc.s_in, sc.lastnz, d_u, num, d_o);
+  count_launch();
+  cudaMemcpyAsync(h_out, d_o, num * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream);
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return MLB_ERR_DRIVER;
+  return MLB_OK;
+}
+
+template <typename Real>
+int seq_total(const void* amp, int n, uint64_t fmask, uint64_t fval, bool fused, int num_sms,
+              cudaStream_t stream, double* total) {
+  SeqScratch sc;
+  uint64_t nc;
+  uint32_t clen;
+  int rc = fused ? seq_prepare<Real, true>(amp, n, fmask, fval, 0, num_sms, stream, sc, nc, clen)
+                 : seq_prepare<Real, false>(amp, n, fmask, fval, 0, num_sms, stream, sc, nc, clen);
+  if (rc) return rc;
+  cudaMemcpyAsync(total, sc.s_in + nc, sizeof(double), cudaMemcpyDeviceToHost, stream);
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return MLB_ERR_DRIVER;
+  return MLB_OK;
+}
+
+}  // namespace
+
+int sample_exact(int dtype, const void* amp, int n, int rule, const double* h_uniforms, size_t num,
+                 uint64_t* h_out, int num_sms, cudaStream_t stream, char* errbuf, size_t errlen) {
+  (void)errbuf;
+  (void)errlen;
+  if (dtype == MLB_C128) return sample_t<double>(amp, n, rule, h_uniforms, num, h_out, num_sms, stream);
+  return sample_t<float>(amp, n, rule, h_uniforms, num, h_out, num_sms, stream);
+}
+
+int seq_sum_exact(int dtype, const void* amp, int n, uint64_t fmask, uint64_t fval, bool fused,
+                  int num_sms, cudaStream_t stream, double* total) {
+  if (dtype == MLB_C128) return seq_total<double>(amp, n, fmask, fval, fused, num_sms, stream, total);
+  return seq_total<float>(amp, n, fmask, fval, fused, num_sms, stream, total);
+}
+
+}  // namespace mlb

@@ -1,0 +1,99 @@
+// mlb_internal.h -- internal types shared by the engine's CUDA kernels and its
+// host runtime.  Not part of the C ABI (include/moonlab_b200.h is).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "moonlab_b200.h"
+
+namespace mlb {
+
+// ---------------------------------------------------------------------------
+// Device-side op encoding.  The host planner lowers mlb_op_t into these
+// "local" ops for one tile pass: qubit positions are rewritten into the
+// tile's local index space (bits 0..L-1 = global bits 0..L-1, bit L+k =
+// global bit high[k]); controls and diagonal qubits outside the tile become
+// per-tile predicates evaluated on the tile's base index.
+// ---------------------------------------------------------------------------
+enum DevOpKind : int32_t {
+  DOP_1Q_GEN = 0,    // generic 2x2 on register bit rt
+  DOP_1Q_REAL = 1,   // real 2x2 (RY-like)
+  DOP_X = 2,         // swap pair
+  DOP_DIAG1 = 3,     // diag(d0, d1) keyed on local bit lt (or outside bit)
+  DOP_PHASE = 4,     // multiply by d0 where (loc & lmask)==lmask (outside part via omask)
+  DOP_ZZ = 5,        // d0 if parity even else d1 over local mask lmask ^ outside parity
+  DOP_2Q_GEN = 6,    // 4x4 on register bits (rt = low, rt2 = high)
+  DOP_SWAP = 7,      // swap bits rt <-> rt2
+  DOP_DENSE = 8,     // dense 2^k block (fused c64); matrix in the pass matrix pool
+};
+
+struct DevOp {
+  int32_t kind;
+  int32_t rt;        // register-group bit of the (low) target
+  int32_t rt2;       // second register-group bit (2Q / SWAP)
+  int32_t lt;        // local bit of the diagonal key (-1: outside the tile)
+  uint32_t lcmask;   // local control mask (tile-local bits)
+  uint32_t lmask;    // local mask (PHASE / ZZ)
+  uint64_t ocmask;   // outside control mask (global bits); op skipped unless all set
+  uint64_t omask;    // outside diagonal mask (global bits): ZZ parity / DIAG1 key / PHASE
+  int32_t k;         // DENSE: number of qubits
+  int32_t mat_off;   // DENSE: offset (in complex entries) into the matrix pool
+  double m[32];      // matrix payload (same layout as mlb_op_t.m)
+};
+
+// One segment = consecutive ops whose non-diagonal targets fit in R
+// register bits; each thread loads a 2^R-amplitude group into registers.
+struct DevSegment {
+  int32_t op_begin, op_end;
+  int32_t nbits;        // number of active register bits (<= R)
+  int32_t bits[5];      // local bit positions of the register bits (ascending)
+};
+
+constexpr int kMaxHigh = 16;
+
+struct DevPass {
+  int32_t n;            // qubits of the state
+  int32_t L;            // low contiguous local bits
+  int32_t H;            // high local bits
+  int32_t num_segments;
+  int32_t high[kMaxHigh];
+  uint64_t num_tiles;   // 2^(n - L - H)
+  uint64_t tile_free_mask; // global bits that enumerate tiles (not in the tile)
+};
+
+// Kernel launchers (kernels_*.cu).  All asynchronous on `stream`.
+int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment* d_segs,
+                     const DevOp* d_ops, const float2* d_mats, int num_sms, cudaStream_t stream);
+int launch_gate(int dtype, void* amp, int n, const mlb_op_t& op, cudaStream_t stream);
+int launch_init_zero(int dtype, void* amp, int n, cudaStream_t stream);
+int launch_convert(int dst_dtype, void* dst, int src_dtype, const void* src, uint64_t dim,
+                   cudaStream_t stream);
+
+// Reductions: results written into a device FP64 scratch block, then copied.
+int launch_reduce_probs_z(int dtype, const void* amp, int n, double* d_out /* n+1 */,
+                          double* d_partials, int num_sms, cudaStream_t stream);
+// Pauli strings sharing one X mask (<= 16 per call); out_terms[t] = Re<P_t>.
+int launch_pauli_group(int dtype, const void* amp, int n, uint64_t xmask, int num_terms,
+                       const uint64_t* d_zmasks, const int* d_nys, double* d_out_terms,
+                       double* d_partials, int num_sms, cudaStream_t stream);
+int launch_probabilities(int dtype, const void* amp, int n, int rule, double* d_out,
+                         cudaStream_t stream);
+int launch_scale(int dtype, void* amp, int n, double factor, uint64_t zero_mask,
+                 uint64_t zero_val, cudaStream_t stream);
+
+// Exact reproduction of the reference's sequential FP64 sums
+// (kernels_sample.cu).  Both synchronize `stream` before returning.
+int sample_exact(int dtype, const void* amp, int n, int rule, const double* h_uniforms,
+                 size_t num, uint64_t* h_out, int num_sms, cudaStream_t stream,
+                 char* errbuf, size_t errlen);
+// Left-to-right sum over indices with (i & fmask) == fval of cabs(a_i)^2:
+// fused = false: s = fl(s + fl(h*h)); fused = true: s = fma(h, h, s).
+int seq_sum_exact(int dtype, const void* amp, int n, uint64_t fmask, uint64_t fval, bool fused,
+                  int num_sms, cudaStream_t stream, double* total);
+
+uint64_t kernel_launch_count();
+void count_launch(uint64_t k = 1);
+
+}  // namespace mlb

@@ -1,0 +1,117 @@
+"""C-ABI surface checks that need no GPU: the library loads, exports every
+function the public headers declare, reports the absence of a device
+cleanly, and plans circuits on the host."""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from moonlab_b200 import _lib, gates_to_ops
+from moonlab_b200.circuits import GATE_DTYPE, brickwork, config_c1, config_c2
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def header_functions():
+    names = set()
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        text = re.sub(r"#[^\n]*", "", text)
+        text = re.sub(r"typedef[^;]*;", "", text)
+        for stmt in text.split(";"):
+            m = re.search(r"\b([A-Za-z_]\w*)\s*\([^()]*\)\s*$", stmt.strip())
+            if m and m.group(1) not in ("if", "while", "sizeof", "enum", "struct"):
+                names.add(m.group(1))
+    return sorted(names)
+
+
+def test_headers_declare_functions():
+    names = header_functions()
+    assert "mlb_state_create" in names and "quantum_state_create_gpu" in names
+    assert len(names) > 60
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    missing = [n for n in header_functions() if not hasattr(lib, n)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_status_strings():
+    lib = _lib.load()
+    assert lib.mlb_status_string(0) == b"ok"
+    assert lib.mlb_status_string(-4) == b"invalid qubit"
+
+
+def _has_gpu():
+    cnt = C.c_int()
+    return _lib.load().mlb_device_count(C.byref(cnt)) == 0 and cnt.value > 0
+
+
+def test_no_device_is_reported_not_faked():
+    if _has_gpu():
+        pytest.skip("a GPU is present")
+    lib = _lib.load()
+    h = C.c_void_p()
+    rc = lib.mlb_state_create(10, 0, 0, C.byref(h))
+    assert rc == -2 and not h.value  # MLB_ERR_NO_DEVICE, no state
+    qs = C.POINTER(_lib.QuantumState)()
+    assert lib.quantum_state_create_gpu(10, C.byref(qs)) == -7  # QS_ERROR_NOT_SUPPORTED
+    assert not qs
+    assert lib.moonlab_cuda_runtime_probe_discrete() in (0, -2)
+
+
+def test_gate_matrices_match_host_libm():
+    th = 0.7312
+    g = np.array([(7, 0, -1, 0, th), (8, 0, -1, 0, th), (9, 0, -1, 0, th), (6, 0, -1, 0, 0.0)],
+                 dtype=GATE_DTYPE)
+    ops = gates_to_ops(g, 1)
+    c, s = math.cos(th / 2.0), math.sin(th / 2.0)
+    assert list(ops[0].m[:8]) == [c, 0.0, 0.0, -s, 0.0, -s, c, 0.0]            # gates.c:392-395
+    assert list(ops[1].m[:8]) == [c, 0.0, -s, 0.0, s, 0.0, c, 0.0]             # gates.c:438-440
+    p0, p1 = complex(math.cos(-th / 2), math.sin(-th / 2)), complex(math.cos(th / 2), math.sin(th / 2))
+    assert list(ops[2].m[:8]) == [p0.real, p0.imag, 0, 0, 0, 0, p1.real, p1.imag]  # gates.c:488-494
+    t = complex(math.cos(math.pi / 4), math.sin(math.pi / 4))
+    assert list(ops[3].m[:8]) == [1, 0, 0, 0, 0, 0, t.real, t.imag]
+
+
+def test_invalid_gate_records_are_rejected():
+    lib = _lib.load()
+    bad = np.array([(10, 3, 3, 0, 0.0)], dtype=GATE_DTYPE)  # control == target
+    cnt = C.c_size_t()
+    rc = lib.mlb_gates_to_ops(bad.ctypes.data_as(C.POINTER(_lib.MlbGate)), 1, 5, None, C.byref(cnt))
+    assert rc == -4
+    bad = np.array([(7, 9, -1, 0, 0.1)], dtype=GATE_DTYPE)  # target outside the register
+    rc = lib.mlb_gates_to_ops(bad.ctypes.data_as(C.POINTER(_lib.MlbGate)), 1, 5, None, C.byref(cnt))
+    assert rc == -4
+
+
+def plan(gates, n, dtype=0, fuse=1):
+    lib = _lib.load()
+    ops = gates_to_ops(gates, n)
+    st = _lib.MlbFlushStats()
+    _lib.check(lib.mlb_plan_ops(ops, len(ops), n, dtype, fuse, C.byref(st)), "mlb_plan_ops")
+    return st
+
+
+def test_planner_groups_the_brickwork_workloads():
+    g1, _ = config_c1()
+    st = plan(g1, 20)
+    assert st.passes <= 20 and st.ops == 572      # 1390 gates, 1q runs fused
+    g2, _ = config_c2()
+    st = plan(g2, 30)
+    assert st.passes <= 80                         # vs 4470 sweeps gate by gate
+    assert st.bytes_moved == st.passes * 2 * 16 * (1 << 30)
+    st64 = plan(g2, 30, dtype=1)
+    assert st64.passes <= st.passes
+
+
+def test_planner_small_state_is_one_pass():
+    st = plan(brickwork(10, 50, 7), 10)
+    assert st.passes == 1
