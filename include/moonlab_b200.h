@@ -174,6 +174,7 @@ typedef struct {
     uint64_t dense_blocks;
     uint64_t bytes_moved;    /* algorithmic HBM bytes of the launched passes */
     uint64_t kernel_launches;
+    uint64_t segments;       /* shared-memory register-group round trips over all passes */
     double   gpu_ms;         /* device time of the flush's kernels (timing enabled), else 0 */
 } mlb_flush_stats_t;
 int  mlb_last_flush_stats(mlb_state_t *s, mlb_flush_stats_t *out);

@@ -388,6 +388,7 @@ struct Planner {
         const uint64_t Q = op_qubits(o), T = op_targets(o);
         if (Q & blocked) { blocked |= Q; if (blocked == allm) break; continue; }
         const uint64_t need = T & ~lowm & ~SH;
+        if (cnt >= kMaxPassOps) break;
         if (need == 0 || (grow && popc(SH | need) <= Hmax)) {
           SH |= need;
           cnt++;
@@ -429,6 +430,73 @@ struct Planner {
     return taken;
   }
 
+  // Reorder a pass's ops (list scheduling) so that ops whose targets fit one
+  // register set run back to back: each segment costs a shared-memory round
+  // trip of the whole tile, so fewer, fuller segments are cheaper.  Two ops
+  // commute when neither's non-diagonal targets touch the other's qubits
+  // (controls and diagonal keys commute with each other); an op may only be
+  // scheduled once every earlier op it does not commute with is scheduled.
+  template <typename LocalMask>
+  std::vector<int> schedule_segments(const std::vector<mlb_op_t>& ops, const std::vector<int>& taken,
+                                     LocalMask&& local_mask, int RB) {
+    const size_t N = taken.size();
+    std::vector<uint32_t> T(N), D(N);
+    std::vector<bool> wide(N);
+    for (size_t i = 0; i < N; i++) {
+      const mlb_op_t& o = ops[taken[i]];
+      uint64_t om;
+      local_mask(op_targets(o), T[i], om);
+      local_mask(op_qubits(o) & ~op_targets(o), D[i], om);
+      wide[i] = o.kind == MLB_OP_2Q;
+    }
+    std::vector<int> blockers(N, 0);
+    std::vector<std::vector<int>> after(N);
+    for (size_t i = 0; i < N; i++)
+      for (size_t j = 0; j < i; j++) {
+        const bool commute = (T[i] & (T[j] | D[j])) == 0 && (T[j] & (T[i] | D[i])) == 0;
+        if (!commute) {
+          blockers[i]++;
+          after[j].push_back((int)i);
+        }
+      }
+    std::vector<bool> done(N, false);
+    std::vector<int> out;
+    out.reserve(N);
+    auto take = [&](size_t i) {
+      done[i] = true;
+      out.push_back(taken[i]);
+      for (int k : after[i]) blockers[k]--;
+    };
+    while (out.size() < N) {
+      uint32_t S = 0;
+      bool any = false;
+      bool progress = true;
+      while (progress) {
+        progress = false;
+        for (size_t i = 0; i < N; i++) {
+          if (done[i] || blockers[i] != 0) continue;
+          if (wide[i]) {  // a generic 4x4 op forms its own segment
+            if (!any) {
+              take(i);
+              any = true;
+              progress = false;
+              break;
+            }
+            continue;
+          }
+          if (popc(S | T[i]) <= RB) {
+            S |= T[i];
+            take(i);
+            any = true;
+            progress = true;
+          }
+        }
+        if (any && !out.empty() && ops[out.back()].kind == MLB_OP_2Q) break;
+      }
+    }
+    return out;
+  }
+
   void lower_pass(const std::vector<mlb_op_t>& ops, const std::vector<int>& taken, int L, uint64_t SH) {
     PlannedPass pp{};
     DevPass& P = pp.pass;
@@ -461,12 +529,36 @@ struct Planner {
           else om |= 1ull << b;
         }
     };
+    const std::vector<int> order = schedule_segments(ops, taken, local_mask, RB);
+    const std::vector<int>& taken_in = taken;
+    (void)taken_in;
+    auto run_segments = [&](const std::vector<int>& taken) {
     size_t i = 0;
     while (i < taken.size()) {
+      // a generic 4x4 op runs alone in a shared-memory segment
+      if (ops[taken[i]].kind == MLB_OP_2Q) {
+        const mlb_op_t& o = ops[taken[i]];
+        DevSegment sg{};
+        sg.mode = 1;
+        sg.nbits = 0;
+        sg.op_begin = (int)dops.size();
+        DevOp d{};
+        std::memcpy(d.m, o.m, sizeof d.m);
+        local_mask(o.cmask, d.lcmask, d.ocmask);
+        d.kind = DOP_2Q_GEN;
+        d.lt = local_of[o.target];
+        d.k = local_of[o.target2];
+        dops.push_back(d);
+        sg.op_end = (int)dops.size();
+        segs.push_back(sg);
+        i++;
+        continue;
+      }
       // grow a segment
       uint32_t bits = 0;
       size_t j = i;
       for (; j < taken.size(); j++) {
+        if (ops[taken[j]].kind == MLB_OP_2Q) break;
         const uint64_t T = op_targets(ops[taken[j]]);
         uint32_t tl = 0;
         uint64_t dummy;
@@ -502,9 +594,8 @@ struct Planner {
             break;
           }
           case MLB_OP_X: d.kind = DOP_X; d.rt = rpos(local_of[o.target]); break;
-          case MLB_OP_2Q:
           case MLB_OP_SWAP:
-            d.kind = o.kind == MLB_OP_2Q ? DOP_2Q_GEN : DOP_SWAP;
+            d.kind = DOP_SWAP;
             d.rt = rpos(local_of[o.target]);
             d.rt2 = rpos(local_of[o.target2]);
             break;
@@ -532,6 +623,8 @@ struct Planner {
       segs.push_back(sg);
       i = j;
     }
+    };
+    run_segments(order);
     pp.seg_end = (int)segs.size();
     P.num_segments = pp.seg_end - pp.seg_begin;
     passes.push_back(pp);
@@ -545,7 +638,7 @@ struct Planner {
       uint64_t SH = 0;
       std::vector<int> taken;
       if ((int)n <= g.TB) {
-        taken = rem;
+        taken.assign(rem.begin(), rem.begin() + std::min<size_t>(rem.size(), kMaxPassOps));
       } else {
         taken = choose(ops, rem, L, SH);
       }
@@ -658,6 +751,7 @@ int flush_impl(mlb_state* s) {
     st.bytes_moved += 2 * ab * dim;
   }
   st.ops = ops.size();
+  st.segments = pl.segs.size();
   if (s->timing) {
     cudaEventRecord(s->t1, s->stream);
     s->timed_pending = true;
@@ -1314,6 +1408,7 @@ int mlb_plan_ops(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fus
   pl.plan(fused);
   mlb_flush_stats_t st{};
   st.passes = pl.passes.size();
+  st.segments = pl.segs.size();
   st.ops = fused.size();
   st.kernel_launches = pl.passes.size();
   st.bytes_moved = st.passes * 2ull * (dtype == MLB_C128 ? 16ull : 8ull) * (1ull << n);

@@ -9,13 +9,15 @@
 //
 // Inside a tile the ops are grouped into segments: consecutive ops whose
 // non-diagonal targets span at most R local bits.  For a segment each
-// thread gathers a 2^R-amplitude group into registers, applies every op of
-// the segment there, and scatters it back: one shared-memory round trip per
-// segment instead of one per gate.  Controls and diagonal phases are
-// evaluated per amplitude from its tile-local index; controls or diagonal
-// qubits that lie outside the tile are constant over the tile and are
-// evaluated once on the tile's base index.  Shared memory is XOR-swizzled on
-// 128-byte rows so that group gathers of any stride are bank-conflict free.
+// thread gathers two 2^R-amplitude groups into registers, applies every op
+// of the segment there (the two groups interleaved for instruction-level
+// parallelism), and scatters them back: one shared-memory round trip per
+// segment instead of one per gate.  The pass's ops are decoded once per CTA
+// into a compact shared-memory program (matrices pre-converted to the state's
+// precision), and the tile-constant part of every op -- controls, phase
+// masks and diagonal keys on qubits outside the tile -- is evaluated once
+// per tile.  Shared memory is XOR-swizzled on 128-byte rows so that group
+// gathers of any stride are bank-conflict free.
 #include <cstdio>
 
 #include "kernels_common.cuh"
@@ -27,20 +29,32 @@ namespace {
 
 template <typename Real> struct TileCfg;
 template <> struct TileCfg<double> {  // complex128: 2^12 amps = 64 KiB per CTA
-  static constexpr int TB = 12, RB = 3, NT = 256, MINB = 2, SW_SHIFT = 3, SW_MASK = 7;
+  static constexpr int TB = 12, RB = 3, NT = 256, MINB = 2, SW_SHIFT = 3, SW_MASK = 7, GPT = 1;
 };
 template <> struct TileCfg<float> {   // complex64: 2^13 amps = 64 KiB per CTA
-  static constexpr int TB = 13, RB = 4, NT = 256, MINB = 2, SW_SHIFT = 4, SW_MASK = 15;
+  static constexpr int TB = 13, RB = 4, NT = 256, MINB = 2, SW_SHIFT = 4, SW_MASK = 15, GPT = 1;
+};
+// GPT: register groups per thread per segment, interleaved for ILP.
+
+template <typename Real>
+__device__ __forceinline__ uint32_t swz(uint32_t e) {
+  return e ^ ((e >> TileCfg<Real>::SW_SHIFT) & TileCfg<Real>::SW_MASK);
+}
+
+// Compact op, decoded into shared memory at kernel start.
+struct SmOp {
+  uint8_t kind, rt, rt2, la;  // register bits (pair/quad), local key bit (31: none)
+  uint8_t lb, ctrl, code, pad1;
+  uint32_t lcmask;             // local control mask
+  uint32_t lmask;              // local mask (PHASE)
+  uint32_t mat;                // op index (matrix slot) or 2Q: global op index
 };
 
-// Tile-local index of register slot k of the current group: the group base
-// with register bit b set for every set bit b of k.  k is a compile-time
-// constant inside the unrolled loops, so this folds to a few ORs.
+// Tile-local index of register slot k of group base gb.
 template <int RB>
-struct Loc {
-  uint32_t gb;
+struct Dep {
   uint32_t bm[RB];
-  __device__ __forceinline__ uint32_t operator()(int k) const {
+  __device__ __forceinline__ uint32_t operator()(uint32_t gb, int k) const {
     uint32_t r = gb;
 #pragma unroll
     for (int b = 0; b < RB; b++)
@@ -49,185 +63,141 @@ struct Loc {
   }
 };
 
-template <typename Real>
-__device__ __forceinline__ uint32_t swz(uint32_t e) {
-  return e ^ ((e >> TileCfg<Real>::SW_SHIFT) & TileCfg<Real>::SW_MASK);
-}
-
-// Apply one non-dense op to the register group.  RT / RT2 are compile-time
-// register-bit positions so the amplitude array stays in registers.
-template <typename Real, int G, int RT, int RBITS = (G == 16 ? 4 : G == 8 ? 3 : G == 4 ? 2 : G == 2 ? 1 : 5)>
-__device__ __forceinline__ void pair_op(typename Cplx<Real>::T (&v)[G], const Loc<RBITS>& loc,
-                                        const DevOp& op) {
-  using A = typename Cplx<Real>::T;
-  const A m00 = ld_m<Real>(op.m, 0), m01 = ld_m<Real>(op.m, 1);
-  const A m10 = ld_m<Real>(op.m, 2), m11 = ld_m<Real>(op.m, 3);
+template <typename A, int G, int RB, int RT, int KIND, bool CTRL, int kGPT>
+__device__ __forceinline__ void op_pair(A (&v)[kGPT][G], const uint32_t (&gb)[kGPT], const Dep<RB>& dep,
+                                        const SmOp& op, const A* __restrict__ M) {
+  A m00, m01, m10, m11;
+  if (KIND != DOP_X) { m00 = M[0]; m01 = M[1]; m10 = M[2]; m11 = M[3]; }
 #pragma unroll
-  for (int k = 0; k < G; k++) {
-    if (k & (1 << RT)) continue;
-    const int k1 = k | (1 << RT);
-    if ((loc(k) & op.lcmask) != op.lcmask) continue;
-    const A a0 = v[k], a1 = v[k1];
-    if (op.kind == DOP_X) {
-      v[k] = a1;
-      v[k1] = a0;
-    } else if (op.kind == DOP_1Q_REAL) {
-      v[k] = {m00.x * a0.x + m01.x * a1.x, m00.x * a0.y + m01.x * a1.y};
-      v[k1] = {m10.x * a0.x + m11.x * a1.x, m10.x * a0.y + m11.x * a1.y};
-    } else {
-      v[k] = cmul2(m00, a0, m01, a1);
-      v[k1] = cmul2(m10, a0, m11, a1);
+  for (int g = 0; g < kGPT; g++) {
+#pragma unroll
+    for (int k = 0; k < G; k++) {
+      if (k & (1 << RT)) continue;
+      const int k1 = k | (1 << RT);
+      if (CTRL && (dep(gb[g], k) & op.lcmask) != op.lcmask) continue;
+      const A a0 = v[g][k], a1 = v[g][k1];
+      if (KIND == DOP_X) {
+        v[g][k] = a1;
+        v[g][k1] = a0;
+      } else if (KIND == DOP_1Q_REAL) {
+        v[g][k] = {m00.x * a0.x + m01.x * a1.x, m00.x * a0.y + m01.x * a1.y};
+        v[g][k1] = {m10.x * a0.x + m11.x * a1.x, m10.x * a0.y + m11.x * a1.y};
+      } else {
+        v[g][k] = cmul2(m00, a0, m01, a1);
+        v[g][k1] = cmul2(m10, a0, m11, a1);
+      }
     }
   }
 }
 
-template <typename Real, int G, int RT, int RT2, int RBITS = (G == 16 ? 4 : G == 8 ? 3 : G == 4 ? 2 : G == 2 ? 1 : 5)>
-__device__ __forceinline__ void quad_op(typename Cplx<Real>::T (&v)[G], const Loc<RBITS>& loc,
-                                        const DevOp& op) {
-  using A = typename Cplx<Real>::T;
+template <typename A, int G, int RB, int RT, int RT2, bool CTRL, int kGPT>
+__device__ __forceinline__ void op_swap(A (&v)[kGPT][G], const uint32_t (&gb)[kGPT], const Dep<RB>& dep,
+                                        const SmOp& op) {
   constexpr int B0 = 1 << RT, B1 = 1 << RT2;
 #pragma unroll
-  for (int k = 0; k < G; k++) {
-    if (k & (B0 | B1)) continue;
-    if ((loc(k) & op.lcmask) != op.lcmask) continue;
-    if (op.kind == DOP_SWAP) {
-      const A t = v[k | B0];
-      v[k | B0] = v[k | B1];
-      v[k | B1] = t;
-      continue;
+  for (int g = 0; g < kGPT; g++) {
+#pragma unroll
+    for (int k = 0; k < G; k++) {
+      if (k & (B0 | B1)) continue;
+      if (CTRL && (dep(gb[g], k) & op.lcmask) != op.lcmask) continue;
+      const A t = v[g][k | B0];  // SWAP
+      v[g][k | B0] = v[g][k | B1];
+      v[g][k | B1] = t;
     }
-    const A x[4] = {v[k], v[k | B0], v[k | B1], v[k | B0 | B1]};
-    A y[4];
+  }
+}
+
+// A generic 4x4 op on local bits (l0 = low index bit, l1), applied directly
+// in shared memory, one quad per thread iteration.
+template <typename Real>
+__device__ __forceinline__ void smem_quad(typename Cplx<Real>::T* sm, uint32_t tile_amps,
+                                          const DevOp& d, int NT) {
+  using A = typename Cplx<Real>::T;
+  const uint32_t l0 = (uint32_t)d.lt, l1 = (uint32_t)d.k;
+  const uint32_t lo = l0 < l1 ? l0 : l1, hi = l0 < l1 ? l1 : l0;
+  const uint32_t b0 = 1u << l0, b1 = 1u << l1;
+  const double* __restrict__ M = d.m;
+  for (uint32_t q = threadIdx.x; q < (tile_amps >> 2); q += NT) {
+    // matrix entries are re-read (L1) per quad: holding all 16 in registers
+    // next to the kernel's amplitude groups would exceed the register budget
+    asm volatile("" ::: "memory");
+    uint32_t i = q;
+    i = ((i >> lo) << (lo + 1)) | (i & ((1u << lo) - 1u));
+    i = ((i >> hi) << (hi + 1)) | (i & ((1u << hi) - 1u));
+    if ((i & d.lcmask) != d.lcmask) continue;
+    const uint32_t idx[4] = {i, i | b0, i | b1, i | b0 | b1};
+    A x[4], y[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) x[c] = sm[swz<Real>(idx[c])];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
       A acc = {0, 0};
 #pragma unroll
       for (int c = 0; c < 4; c++) {
-        const A mm = ld_m<Real>(op.m, r * 4 + c);
-        acc.x += mm.x * x[c].x - mm.y * x[c].y;
-        acc.y += mm.x * x[c].y + mm.y * x[c].x;
+        const Real mr = (Real)M[(r * 4 + c) * 2], mi = (Real)M[(r * 4 + c) * 2 + 1];
+        acc.x += mr * x[c].x - mi * x[c].y;
+        acc.y += mr * x[c].y + mi * x[c].x;
       }
       y[r] = acc;
     }
-    v[k] = y[0];
-    v[k | B0] = y[1];
-    v[k | B1] = y[2];
-    v[k | B0 | B1] = y[3];
+#pragma unroll
+    for (int c = 0; c < 4; c++) sm[swz<Real>(idx[c])] = y[c];
   }
 }
 
-template <typename Real, int G, int RBITS = (G == 16 ? 4 : G == 8 ? 3 : G == 4 ? 2 : G == 2 ? 1 : 5)>
-__device__ __forceinline__ void diag_op(typename Cplx<Real>::T (&v)[G], const Loc<RBITS>& loc,
-                                        const DevOp& op, uint64_t tile_base) {
-  using A = typename Cplx<Real>::T;
-  const A d0 = ld_m<Real>(op.m, 0), d1 = ld_m<Real>(op.m, 1);
-  if (op.kind == DOP_PHASE) {
-    if ((tile_base & op.omask) != op.omask) return;
+// DIAG1 / ZZ: f = M[key], key = bit la (xor bit lb) of the local index xor
+// the tile-constant key.  PHASE: multiply by M[0] where the local mask holds.
+template <typename A, int G, int RB, bool PHASE, bool CTRL, int kGPT>
+__device__ __forceinline__ void op_diag(A (&v)[kGPT][G], const uint32_t (&gb)[kGPT], const Dep<RB>& dep,
+                                        const SmOp& op, const A* __restrict__ M, uint32_t tkey) {
+  const A d0 = M[0], d1 = M[1];
 #pragma unroll
-    for (int k = 0; k < G; k++)
-      if ((loc(k) & op.lmask) == op.lmask) v[k] = cmul(d0, v[k]);
-  } else if (op.kind == DOP_DIAG1) {
-    const int out_bit = (tile_base & op.omask) ? 1 : 0;
+  for (int g = 0; g < kGPT; g++) {
 #pragma unroll
     for (int k = 0; k < G; k++) {
-      if ((loc(k) & op.lcmask) != op.lcmask) continue;
-      const int b = op.lt >= 0 ? (int)((loc(k) >> op.lt) & 1u) : out_bit;
-      v[k] = cmul(b ? d1 : d0, v[k]);
-    }
-  } else {  // DOP_ZZ
-    const int po = parity64(tile_base & op.omask);
-#pragma unroll
-    for (int k = 0; k < G; k++) {
-      const int par = (__popc(loc(k) & op.lmask) & 1) ^ po;
-      v[k] = cmul(par ? d1 : d0, v[k]);
+      const uint32_t loc = dep(gb[g], k);
+      if (PHASE) {
+        if ((loc & op.lmask) == op.lmask) v[g][k] = cmul(d0, v[g][k]);
+      } else {
+        if (CTRL && (loc & op.lcmask) != op.lcmask) continue;
+        const uint32_t key = ((loc >> op.la) ^ (loc >> op.lb) ^ tkey) & 1u;
+        v[g][k] = cmul(key ? d1 : d0, v[g][k]);
+      }
     }
   }
 }
 
-// Dense 2^nb x 2^nb block on the whole register group (complex64 fused path,
-// CUDA-core version).  Matrix rows/cols follow the register-bit order.
-template <typename Real, int G>
-__device__ __forceinline__ void dense_op(typename Cplx<Real>::T (&v)[G], int nb,
-                                         const DevOp& op, const float2* __restrict__ mats) {
-  using A = typename Cplx<Real>::T;
-  const int d = 1 << nb;
-  const float2* M = mats + op.mat_off;
-  A y[G];
-#pragma unroll
-  for (int r = 0; r < G; r++) {
-    A acc = {0, 0};
-    if (r < d) {
-#pragma unroll
-      for (int c = 0; c < G; c++) {
-        if (c < d) {
-          const float2 mm = __ldg(&M[r * d + c]);
-          acc.x += (Real)mm.x * v[c].x - (Real)mm.y * v[c].y;
-          acc.y += (Real)mm.x * v[c].y + (Real)mm.y * v[c].x;
-        }
-      }
-    }
-    y[r] = acc;
-  }
-#pragma unroll
-  for (int r = 0; r < G; r++)
-    if (r < d) v[r] = y[r];
-}
-
-template <typename Real, int G, int RBITS = (G == 16 ? 4 : G == 8 ? 3 : G == 4 ? 2 : G == 2 ? 1 : 5)>
-__device__ __forceinline__ void apply_op(typename Cplx<Real>::T (&v)[G], const Loc<RBITS>& loc,
-                                      const DevOp& op, uint64_t tile_base, int nb,
-                                      const float2* __restrict__ mats) {
-  switch (op.kind) {
-    case DOP_1Q_GEN:
-    case DOP_1Q_REAL:
-    case DOP_X:
-      switch (op.rt) {
-        case 0: pair_op<Real, G, 0>(v, loc, op); break;
-        case 1: if constexpr (G > 2) pair_op<Real, G, 1>(v, loc, op); break;
-        case 2: if constexpr (G > 4) pair_op<Real, G, 2>(v, loc, op); break;
-        case 3: if constexpr (G > 8) pair_op<Real, G, 3>(v, loc, op); break;
-        case 4: if constexpr (G > 16) pair_op<Real, G, 4>(v, loc, op); break;
-      }
-      break;
-    case DOP_2Q_GEN:
-    case DOP_SWAP: {
-      const int code = op.rt * 8 + op.rt2;
-#define MLB_Q(a, b) \
-  case a * 8 + b:   \
-    if constexpr (G > (1 << a) && G > (1 << b)) quad_op<Real, G, a, b>(v, loc, op); \
-    break;
-      switch (code) {
-        MLB_Q(0, 1) MLB_Q(0, 2) MLB_Q(0, 3) MLB_Q(1, 0) MLB_Q(1, 2) MLB_Q(1, 3)
-        MLB_Q(2, 0) MLB_Q(2, 1) MLB_Q(2, 3) MLB_Q(3, 0) MLB_Q(3, 1) MLB_Q(3, 2)
-      }
-#undef MLB_Q
-      break;
-    }
-    case DOP_DIAG1:
-    case DOP_PHASE:
-    case DOP_ZZ:
-      diag_op<Real, G>(v, loc, op, tile_base);
-      break;
-    case DOP_DENSE:
-      dense_op<Real, G>(v, nb, op, mats);
-      break;
-  }
-}
+// Dispatch code of an op: one switch selects a fully specialised routine.
+//   pair ops:  (kind 0..2) * 16 + rt * 2 + ctrl          -> 0 .. 47
+//   swap:      64 + (rt * 4 + rt2) * 2 + ctrl            -> 64 .. 95
+//   diag:      96 + phase * 2 + ctrl                     -> 96 .. 99
+__host__ __device__ constexpr int code_pair(int kind, int rt, int ctrl) { return kind * 16 + rt * 2 + ctrl; }
+__host__ __device__ constexpr int code_swap(int rt, int rt2, int ctrl) { return 64 + (rt * 4 + rt2) * 2 + ctrl; }
+__host__ __device__ constexpr int code_diag(int phase, int ctrl) { return 96 + phase * 2 + ctrl; }
 
 template <typename Real>
 __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
     k_tile(typename Cplx<Real>::T* __restrict__ amp, const DevPass pass,
-           const DevSegment* __restrict__ segs, const DevOp* __restrict__ ops,
-           const float2* __restrict__ mats) {
+           const DevSegment* __restrict__ segs, const DevOp* __restrict__ ops) {
   using A = typename Cplx<Real>::T;
-  constexpr int NT = TileCfg<Real>::NT, RB = TileCfg<Real>::RB, G = 1 << RB;
+  constexpr int NT = TileCfg<Real>::NT, RB = TileCfg<Real>::RB, G = 1 << RB, kGPT = TileCfg<Real>::GPT;
+  constexpr int TB = TileCfg<Real>::TB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A* sm = reinterpret_cast<A*>(smem_raw);
   __shared__ uint64_t rowoff[1 << (TileCfg<Real>::TB - 5)];
+  __shared__ SmOp sops[kMaxPassOps];
+  __shared__ A smat[kMaxPassOps][4];
+  __shared__ uint8_t ton[kMaxPassOps];
+  __shared__ uint8_t tkey[kMaxPassOps];
+  __shared__ DevSegment ssegs[kMaxPassSegs];
 
   const int L = pass.L, H = pass.H;
   const uint32_t tile_amps = 1u << (L + H);
   const uint32_t lmask_low = (1u << L) - 1u;
+  const int nseg = pass.num_segments;
+  const int op0 = segs[0].op_begin, nops = segs[nseg - 1].op_end - op0;
+
+  // ---- prologue: row offsets, compact program ----
   for (uint32_t r = threadIdx.x; r < (1u << H); r += NT) {
     uint64_t off = 0;
 #pragma unroll
@@ -235,53 +205,160 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
       if (k < H && (r >> k & 1u)) off |= 1ull << pass.high[k];
     rowoff[r] = off;
   }
+  for (int s = threadIdx.x; s < nseg; s += NT) {
+    DevSegment sg = segs[s];
+    sg.op_begin -= op0;
+    sg.op_end -= op0;
+    ssegs[s] = sg;
+  }
+  for (int o = threadIdx.x; o < nops; o += NT) {
+    const DevOp& d = ops[op0 + o];
+    SmOp so;
+    so.kind = (uint8_t)d.kind;
+    so.rt = (uint8_t)(d.rt < 0 ? 0 : d.rt);
+    so.rt2 = (uint8_t)(d.rt2 < 0 ? 0 : d.rt2);
+    so.la = 31;
+    so.lb = 31;
+    so.ctrl = d.lcmask != 0;
+    so.lcmask = d.lcmask;
+    so.lmask = d.lmask;
+    so.mat = (uint32_t)(op0 + o);
+    if (d.kind == DOP_1Q_GEN || d.kind == DOP_1Q_REAL || d.kind == DOP_X)
+      so.code = (uint8_t)code_pair(d.kind, so.rt, so.ctrl);
+    else if (d.kind == DOP_SWAP)
+      so.code = (uint8_t)code_swap(so.rt, so.rt2, so.ctrl);
+    else
+      so.code = (uint8_t)code_diag(d.kind == DOP_PHASE ? 1 : 0, so.ctrl);
+    if (d.kind == DOP_DIAG1) {
+      so.la = d.lt >= 0 ? (uint8_t)d.lt : 31;
+    } else if (d.kind == DOP_ZZ) {
+      // up to two local bits of lmask; the rest is tile-constant parity
+      uint32_t lm = d.lmask;
+      if (lm) { so.la = (uint8_t)(__ffs(lm) - 1); lm &= lm - 1; }
+      if (lm) { so.lb = (uint8_t)(__ffs(lm) - 1); }
+    }
+    sops[o] = so;
+#pragma unroll
+    for (int k = 0; k < 4; k++) smat[o][k] = A{(Real)d.m[2 * k], (Real)d.m[2 * k + 1]};
+  }
   __syncthreads();
 
   for (uint64_t tile = blockIdx.x; tile < pass.num_tiles; tile += gridDim.x) {
     const uint64_t tile_base = pdep64(tile, pass.tile_free_mask);
-    // HBM -> shared (coalesced rows of 2^L amplitudes)
-#pragma unroll 4
-    for (uint32_t e = threadIdx.x; e < tile_amps; e += NT) {
-      const uint64_t g = tile_base | rowoff[e >> L] | (e & lmask_low);
-      sm[swz<Real>(e)] = amp[g];
+    // tile-constant op predicates and keys
+    for (int o = threadIdx.x; o < nops; o += NT) {
+      const DevOp& d = ops[op0 + o];
+      bool on = (tile_base & d.ocmask) == d.ocmask;
+      uint32_t key = 0;
+      if (d.kind == DOP_PHASE) on = on && ((tile_base & d.omask) == d.omask);
+      else key = (uint32_t)(__popcll(tile_base & d.omask) & 1);
+      ton[o] = on;
+      tkey[o] = (uint8_t)key;
+    }
+    // HBM -> shared (coalesced rows of 2^L amplitudes).  A full tile has a
+    // compile-time trip count, so all of a thread's loads are in flight at once.
+    if (tile_amps == (1u << TB)) {
+      constexpr int PER = (1 << TB) / NT;
+      A tmp[PER];
+#pragma unroll
+      for (int j = 0; j < PER; j++) {
+        const uint32_t e = threadIdx.x + j * NT;
+        tmp[j] = __ldcs(&amp[tile_base | rowoff[e >> L] | (e & lmask_low)]);
+      }
+#pragma unroll
+      for (int j = 0; j < PER; j++) sm[swz<Real>(threadIdx.x + j * NT)] = tmp[j];
+    } else {
+      for (uint32_t e = threadIdx.x; e < tile_amps; e += NT) {
+        const uint64_t gidx = tile_base | rowoff[e >> L] | (e & lmask_low);
+        sm[swz<Real>(e)] = amp[gidx];
+      }
     }
     __syncthreads();
 
-    for (int s = 0; s < pass.num_segments; s++) {
-      const DevSegment& seg = segs[s];
+    for (int s = 0; s < nseg; s++) {
+      const DevSegment& seg = ssegs[s];
+      if (seg.mode == 1) {
+        const int o = seg.op_begin;
+        if (ton[o]) smem_quad<Real>(sm, tile_amps, ops[op0 + o], NT);
+        __syncthreads();
+        continue;
+      }
       const int nb = seg.nbits;
-      Loc<RB> lc;
+      Dep<RB> dep;
 #pragma unroll
-      for (int b = 0; b < RB; b++) lc.bm[b] = b < nb ? (1u << seg.bits[b]) : 0u;
+      for (int b = 0; b < RB; b++) dep.bm[b] = b < nb ? (1u << seg.bits[b]) : 0u;
       const uint32_t groups = tile_amps >> nb;
-      for (uint32_t gi = threadIdx.x; gi < groups; gi += NT) {
-        uint32_t gb = gi;
-        for (int b = 0; b < nb; b++) {
-          const uint32_t p = seg.bits[b];
-          gb = ((gb >> p) << (p + 1)) | (gb & ((1u << p) - 1u));
-        }
-        lc.gb = gb;
-        A v[G];
+      for (uint32_t g0 = threadIdx.x; g0 < groups; g0 += NT * kGPT) {
+        uint32_t gb[kGPT];
+        bool valid[kGPT];
+        A v[kGPT][G];
 #pragma unroll
-        for (int k = 0; k < G; k++)
-          if (k < (1 << nb)) v[k] = sm[swz<Real>(lc(k))];
+        for (int g = 0; g < kGPT; g++) {
+          const uint32_t gi = g0 + g * NT;
+          valid[g] = gi < groups;
+          uint32_t x = valid[g] ? gi : g0;
+          for (int b = 0; b < nb; b++) {
+            const uint32_t p = seg.bits[b];
+            x = ((x >> p) << (p + 1)) | (x & ((1u << p) - 1u));
+          }
+          gb[g] = x;
+#pragma unroll
+          for (int k = 0; k < G; k++)
+            if (k < (1 << nb)) v[g][k] = sm[swz<Real>(dep(x, k))];
+        }
         for (int o = seg.op_begin; o < seg.op_end; o++) {
-          const DevOp& op = ops[o];
-          if ((tile_base & op.ocmask) != op.ocmask) continue;
-          apply_op<Real, G>(v, lc, op, tile_base, nb, mats);
+          if (!ton[o]) continue;
+          const SmOp op = sops[o];
+          const A* M = smat[o];
+          switch (op.code) {
+#define MLB_P(kind, rt, c)                                                                       \
+  case code_pair(kind, rt, c):                                                                   \
+    if constexpr (RB > rt) op_pair<A, G, RB, rt, kind, (bool)c, kGPT>(v, gb, dep, op, M);         \
+    break;
+#define MLB_PK(kind) MLB_P(kind, 0, 0) MLB_P(kind, 0, 1) MLB_P(kind, 1, 0) MLB_P(kind, 1, 1) \
+                     MLB_P(kind, 2, 0) MLB_P(kind, 2, 1) MLB_P(kind, 3, 0) MLB_P(kind, 3, 1)
+            MLB_PK(DOP_1Q_GEN) MLB_PK(DOP_1Q_REAL) MLB_PK(DOP_X)
+#define MLB_S(a, b, c)                                                                       \
+  case code_swap(a, b, c):                                                                   \
+    if constexpr (RB > a && RB > b && a != b) op_swap<A, G, RB, a, b, (bool)c, kGPT>(v, gb, dep, op); \
+    break;
+#define MLB_SS(a, b) MLB_S(a, b, 0) MLB_S(a, b, 1)
+            MLB_SS(0, 1) MLB_SS(0, 2) MLB_SS(0, 3) MLB_SS(1, 0) MLB_SS(1, 2) MLB_SS(1, 3)
+            MLB_SS(2, 0) MLB_SS(2, 1) MLB_SS(2, 3) MLB_SS(3, 0) MLB_SS(3, 1) MLB_SS(3, 2)
+            case code_diag(0, 0): op_diag<A, G, RB, false, false, kGPT>(v, gb, dep, op, M, tkey[o]); break;
+            case code_diag(0, 1): op_diag<A, G, RB, false, true, kGPT>(v, gb, dep, op, M, tkey[o]); break;
+            case code_diag(1, 0): op_diag<A, G, RB, true, false, kGPT>(v, gb, dep, op, M, tkey[o]); break;
+            case code_diag(1, 1): op_diag<A, G, RB, true, false, kGPT>(v, gb, dep, op, M, tkey[o]); break;
+#undef MLB_P
+#undef MLB_PK
+#undef MLB_S
+#undef MLB_SS
+          }
         }
 #pragma unroll
-        for (int k = 0; k < G; k++)
-          if (k < (1 << nb)) sm[swz<Real>(lc(k))] = v[k];
+        for (int g = 0; g < kGPT; g++) {
+          if (!valid[g]) continue;
+#pragma unroll
+          for (int k = 0; k < G; k++)
+            if (k < (1 << nb)) sm[swz<Real>(dep(gb[g], k))] = v[g][k];
+        }
       }
       __syncthreads();
     }
 
-    // shared -> HBM
-#pragma unroll 4
-    for (uint32_t e = threadIdx.x; e < tile_amps; e += NT) {
-      const uint64_t g = tile_base | rowoff[e >> L] | (e & lmask_low);
-      amp[g] = sm[swz<Real>(e)];
+    // shared -> HBM (streaming stores: the state is far larger than L2)
+    if (tile_amps == (1u << TB)) {
+      constexpr int PER = (1 << TB) / NT;
+#pragma unroll
+      for (int j = 0; j < PER; j++) {
+        const uint32_t e = threadIdx.x + j * NT;
+        __stcs(&amp[tile_base | rowoff[e >> L] | (e & lmask_low)], sm[swz<Real>(e)]);
+      }
+    } else {
+      for (uint32_t e = threadIdx.x; e < tile_amps; e += NT) {
+        const uint64_t gidx = tile_base | rowoff[e >> L] | (e & lmask_low);
+        amp[gidx] = sm[swz<Real>(e)];
+      }
     }
     __syncthreads();
   }
@@ -289,7 +366,7 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
 
 template <typename Real>
 int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, const DevOp* d_ops,
-                  const float2* d_mats, int num_sms, cudaStream_t stream) {
+                  int num_sms, cudaStream_t stream) {
   using A = typename Cplx<Real>::T;
   constexpr int NT = TileCfg<Real>::NT;
   const size_t smem = sizeof(A) << (pass.L + pass.H);
@@ -304,8 +381,7 @@ int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, cons
   if (per_sm < 1) per_sm = 1;
   uint64_t grid = (uint64_t)num_sms * per_sm;
   if (grid > pass.num_tiles) grid = pass.num_tiles;
-  k_tile<Real><<<(unsigned)grid, NT, smem, stream>>>(reinterpret_cast<A*>(amp), pass, d_segs,
-                                                     d_ops, d_mats);
+  k_tile<Real><<<(unsigned)grid, NT, smem, stream>>>(reinterpret_cast<A*>(amp), pass, d_segs, d_ops);
   count_launch();
   return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
 }
@@ -314,9 +390,10 @@ int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, cons
 
 int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment* d_segs,
                      const DevOp* d_ops, const float2* d_mats, int num_sms, cudaStream_t stream) {
-  if (dtype == MLB_C128)
-    return launch_tile_t<double>(amp, pass, d_segs, d_ops, d_mats, num_sms, stream);
-  return launch_tile_t<float>(amp, pass, d_segs, d_ops, d_mats, num_sms, stream);
+  (void)d_mats;
+  if (pass.num_segments < 1 || pass.num_segments > kMaxPassSegs) return MLB_ERR_INVALID_ARG;
+  if (dtype == MLB_C128) return launch_tile_t<double>(amp, pass, d_segs, d_ops, num_sms, stream);
+  return launch_tile_t<float>(amp, pass, d_segs, d_ops, num_sms, stream);
 }
 
 }  // namespace mlb

@@ -38,7 +38,7 @@ struct DevOp {
   uint32_t lmask;    // local mask (PHASE / ZZ)
   uint64_t ocmask;   // outside control mask (global bits); op skipped unless all set
   uint64_t omask;    // outside diagonal mask (global bits): ZZ parity / DIAG1 key / PHASE
-  int32_t k;         // DENSE: number of qubits
+  int32_t k;         // DENSE: number of qubits; 2Q (shared-memory segment): local bit of target2
   int32_t mat_off;   // DENSE: offset (in complex entries) into the matrix pool
   double m[32];      // matrix payload (same layout as mlb_op_t.m)
 };
@@ -48,10 +48,15 @@ struct DevOp {
 struct DevSegment {
   int32_t op_begin, op_end;
   int32_t nbits;        // number of active register bits (<= R)
-  int32_t bits[5];      // local bit positions of the register bits (ascending)
+  int32_t bits[4];      // local bit positions of the register bits (ascending)
+  int32_t mode;         // 0: register groups; 1: one generic 4x4 op applied in shared memory
 };
 
 constexpr int kMaxHigh = 16;
+// A pass's op program is decoded into shared memory; the planner keeps every
+// pass within these sizes.
+constexpr int kMaxPassOps = 160;
+constexpr int kMaxPassSegs = 160;
 
 struct DevPass {
   int32_t n;            // qubits of the state

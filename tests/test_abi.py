@@ -112,6 +112,10 @@ def test_planner_groups_the_brickwork_workloads():
     assert st64.passes <= st.passes
 
 
-def test_planner_small_state_is_one_pass():
+def test_planner_small_state_single_tile():
+    # the whole 10-qubit state is one tile: passes only split the op program
+    # into shared-memory-sized chunks (160 ops)
     st = plan(brickwork(10, 50, 7), 10)
+    assert st.passes == -(-st.ops // 160)
+    st = plan(brickwork(10, 5, 7), 10)
     assert st.passes == 1

@@ -223,7 +223,9 @@ def _states(n):
     uniform = np.full(d, 1 / np.sqrt(d), complex)
     rnd = rng.standard_normal(d) + 1j * rng.standard_normal(d)
     rnd /= np.linalg.norm(rnd)
-    sparse = np.where(rng.random(d) < 0.05, rnd, 0)
+    keep = rng.random(d) < 0.05
+    keep[rng.integers(0, d, 3)] = True  # never empty
+    sparse = np.where(keep, rnd, 0)
     sparse /= np.linalg.norm(sparse)
     tiny = rnd * np.exp(-rng.uniform(0, 300, d))  # probabilities down to ~1e-260
     tiny[d // 2] = 1.0
@@ -370,8 +372,13 @@ def test_reference_core_routes_to_engine(gpu):
     import os
     _lib.load()  # RTLD_GLOBAL first
     core = C.CDLL(str(B.REF_DROPIN_LIB), mode=os.RTLD_GLOBAL)
+    # A program calling quantum_state_create_gpu resolves it in the global
+    # scope, where the engine's strong definition (loaded first) precedes the
+    # reference's weak stub (state.c:645-651); dlsym on the core's own handle
+    # would return the stub instead.
+    glob = C.CDLL(None)
     sp = C.POINTER(_lib.QuantumState)
-    core.quantum_state_create_gpu.argtypes = [C.c_size_t, C.POINTER(sp)]
+    glob.quantum_state_create_gpu.argtypes = [C.c_size_t, C.POINTER(sp)]
     for name in ("gate_rx", "gate_ry", "gate_rz"):
         getattr(core, name).argtypes = [sp, C.c_int, C.c_double]
     core.gate_cnot.argtypes = [sp, C.c_int, C.c_int]
@@ -382,7 +389,7 @@ def test_reference_core_routes_to_engine(gpu):
     core.quantum_state_destroy.argtypes = [sp]
     n = 12
     qs = sp()
-    assert core.quantum_state_create_gpu(n, C.byref(qs)) == 0
+    assert glob.quantum_state_create_gpu(n, C.byref(qs)) == 0
     assert qs.contents.gpu_backend == 1
     g = brickwork(n, 6, 31)
     for rec in g:
