@@ -187,6 +187,29 @@ int  mlb_plan_ops(const mlb_op_t *ops, size_t num_ops, uint32_t num_qubits, int 
                   int fuse1q, mlb_flush_stats_t *out);
 int  mlb_total_kernel_launches(uint64_t *out);
 
+/* ---- batched adjoint gradient (hardware-efficient ansatz) ---------------- */
+/* Energy E(theta) = <psi|H|psi> and dE/dtheta for the tape of
+ * vqe_build_hea_diff_circuit (vqe.c:1946-1981): X on the set bits of
+ * hf_reference, then per layer RY(q, theta[2(lN+q)]), RZ(q, theta[2(lN+q)+1])
+ * for every qubit and the CNOT(q, q+1) ladder.  H = sum_k c_k P_k with P_k
+ * given by its X mask (X or Y qubits) and Z mask (Z or Y qubits).  The
+ * gradient equals moonlab_diff_backward_pauli_sum's (differentiable.c:478). */
+typedef struct mlb_hea mlb_hea_t;
+int  mlb_hea_create(uint32_t num_qubits, uint32_t num_layers, uint64_t hf_reference,
+                    size_t num_terms, const uint64_t *xmasks, const uint64_t *zmasks,
+                    const double *coeffs, int dtype, int device, mlb_hea_t **out);
+void mlb_hea_free(mlb_hea_t *h);
+int  mlb_hea_num_parameters(const mlb_hea_t *h, uint32_t *out);
+/* B parameter vectors params[B][P] -> energies[B] and grads[B][P] (either may
+ * be NULL).  on_device = 1: all three are device pointers. */
+int  mlb_hea_evaluate(mlb_hea_t *h, size_t batch, const double *params, double *energies,
+                      double *grads, int on_device);
+/* psi + lambda bytes allowed per sub-batch (0 = 80% of free device memory). */
+int  mlb_hea_set_memory_budget(mlb_hea_t *h, size_t bytes);
+int  mlb_hea_plan_stats(const mlb_hea_t *h, uint32_t *fwd_passes, uint32_t *lambda_passes,
+                        uint32_t *bwd_passes);
+const char *mlb_hea_last_error(void);
+
 /* ---- error text ---------------------------------------------------------- */
 const char *mlb_status_string(int status);
 const char *mlb_last_error(void);   /* thread-local detail of the last failure */

@@ -96,6 +96,19 @@ int moonlab_cuda_runtime_probe_discrete(void);
 /* cuda_statevec.cu:418 -- device = local_rank mod device count */
 int moonlab_cuda_select_device_for_rank(int local_rank, int *device_id, int *device_count);
 
+/* ---- VQE gradient (src/applications/moonlab_export.h:1319, definition
+ *      src/applications/moonlab_vqe_export.c:27-42).  solver is the
+ *      reference's vqe_solver_t (src/algorithms/vqe.h:545-568).  Returns 0 ok,
+ *      -1 NULL argument, -2 num_parameters != ansatz->num_parameters, -3
+ *      failure: noise model enabled (no exact gradient, as the reference's
+ *      exact-or-error contract), an ansatz other than the hardware-efficient
+ *      one, or a device error.  The batched variant takes params[B][P] and
+ *      writes grads[B][P] with the same codes. ---- */
+int moonlab_vqe_gradient(void *solver, const double *parameters, double *gradient_out,
+                         size_t num_parameters);
+int moonlab_b200_vqe_gradient_batch(void *solver, size_t batch, const double *parameters,
+                                    double *gradients_out, size_t num_parameters);
+
 /* The engine handle behind a GPU-backed quantum_state_t (for callers that
  * want the engine's FP64 reductions, sampling and collapse directly). */
 struct mlb_state *moonlab_b200_engine_of(quantum_state_t *state);

@@ -111,6 +111,19 @@ _SIGS = {
     "mlb_plan_ops": (C.c_int, [C.POINTER(MlbOp), C.c_size_t, C.c_uint32, C.c_int, C.c_int,
                                C.POINTER(MlbFlushStats)]),
     "mlb_total_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),
+    "mlb_hea_create": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_size_t, C.POINTER(C.c_uint64),
+                                 C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_int, C.c_int,
+                                 C.POINTER(C.c_void_p)]),
+    "mlb_hea_free": (None, [C.c_void_p]),
+    "mlb_hea_num_parameters": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "mlb_hea_evaluate": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "mlb_hea_set_memory_budget": (C.c_int, [C.c_void_p, C.c_size_t]),
+    "mlb_hea_plan_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                     C.POINTER(C.c_uint32)]),
+    "mlb_hea_last_error": (C.c_char_p, []),
+    "moonlab_vqe_gradient": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_size_t]),
+    "moonlab_b200_vqe_gradient_batch": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_double),
+                                                  C.POINTER(C.c_double), C.c_size_t]),
     "mlb_status_string": (C.c_char_p, [C.c_int]),
     "mlb_last_error": (C.c_char_p, []),
     # reference-compatible drop-in surface

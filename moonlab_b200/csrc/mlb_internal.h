@@ -68,6 +68,52 @@ struct DevPass {
   uint64_t tile_free_mask; // global bits that enumerate tiles (not in the tile)
 };
 
+// ---------------------------------------------------------------------------
+// Adjoint-gradient passes (kernels_adjoint.cu).  A pass covers a batch of
+// states stored back to back, [B][2^n]; tiles never span two states.
+// ---------------------------------------------------------------------------
+constexpr int kMaxAdjOps = 160;
+constexpr int kMaxAdjSegs = 64;
+constexpr int kMaxAdjSlots = 96;   // parameter gradients accumulated per pass
+constexpr int kMaxAdjTerms = 128;  // Pauli terms per lambda pass
+enum AdjKind : int32_t { ADJ_KIND_X = 0, ADJ_KIND_RY = 1, ADJ_KIND_RZ = 2 };
+
+struct AdjOp {
+  int32_t kind;      // ADJ_KIND_*; X with a control mask is CNOT
+  int32_t rt;        // register bit of the target (X, RY)
+  int32_t lt;        // RZ: local bit of the target, -1 when outside the tile
+  int32_t qt;        // RZ: global target qubit (tile-constant key when outside)
+  int32_t p;         // parameter index (RY, RZ), -1 otherwise
+  int32_t slot;      // backward: gradient slot of this pass, -1 none
+  uint32_t lcmask;   // local control mask (CNOT control inside the tile)
+  uint32_t pad;
+  uint64_t ocmask;   // outside control mask (global bits)
+};
+struct AdjSeg {
+  int32_t op_begin, op_end;
+  int32_t bits[3];   // register bits (ascending local bit positions)
+};
+struct AdjTerm {     // one Pauli string restricted to a tile
+  uint32_t xl, zl;   // local X / Z masks
+  uint64_t zo;       // Z mask outside the tile (global bits)
+  double cr, ci;     // c_k * i^{#Y}
+};
+struct AdjPass {
+  int32_t n, L, H;
+  int32_t num_ops, num_segments, num_slots, num_params;
+  int32_t high[kMaxHigh];
+  uint64_t tiles_per_state, num_tiles, tile_free_mask;
+  AdjSeg segs[kMaxAdjSegs];
+};
+int adj_tile_bits(int dtype, bool dual);
+int launch_adj_init(int dtype, void* psi, int n, uint64_t batch, uint64_t hf, cudaStream_t stream);
+int launch_adj_gates(int dtype, void* psi, void* lam, const AdjPass& P, const AdjOp* d_ops, const double2* d_cs,
+                     double* d_partials, bool dual, bool backward, int num_sms, cudaStream_t stream);
+int launch_adj_pauli(int dtype, const void* psi, void* lam, const AdjPass& P, const AdjTerm* d_terms,
+                     bool accumulate, bool energy, double* d_epart, int num_sms, cudaStream_t stream);
+int launch_adj_reduce(const double* d_partials, uint64_t tiles_per_state, int num_slots, uint64_t batch,
+                      const int* d_param_of_slot, int num_params, double* d_out, cudaStream_t stream);
+
 // Kernel launchers (kernels_*.cu).  All asynchronous on `stream`.
 int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment* d_segs,
                      const DevOp* d_ops, const float2* d_mats, int num_sms, cudaStream_t stream);

@@ -1,0 +1,345 @@
+// planner.h -- groups a gate-op sequence into tile passes and, inside a
+// pass, into register-group segments (used by the state engine and by the
+// adjoint-gradient engine).  Host-only.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "mlb_internal.h"
+
+namespace mlb {
+namespace plan {
+
+inline int popc(uint64_t x) { return __builtin_popcountll(x); }
+
+// Tile geometry per dtype (must match TileCfg in kernels_tile.cu).
+struct Geo {
+  int TB, RB;
+};
+inline Geo geo(int dtype) { return dtype == MLB_C128 ? Geo{12, 3} : Geo{13, 4}; }
+
+// Non-diagonal target qubits of an op (must lie inside a tile) and all the
+// qubits it touches (targets, controls, diagonal keys).
+inline uint64_t op_targets(const mlb_op_t& o) {
+  switch (o.kind) {
+    case MLB_OP_1Q:
+    case MLB_OP_X: return 1ull << o.target;
+    case MLB_OP_2Q:
+    case MLB_OP_SWAP: return (1ull << o.target) | (1ull << o.target2);
+    default: return 0;  // diagonal
+  }
+}
+inline uint64_t op_qubits(const mlb_op_t& o) {
+  uint64_t q = o.cmask | op_targets(o);
+  if (o.kind == MLB_OP_DIAG1) q |= 1ull << o.target;
+  if (o.kind == MLB_OP_ZZ) q |= (1ull << o.target) | (1ull << o.target2);
+  return q;
+}
+
+// ---------------------------------------------------------------------------
+// planner
+// ---------------------------------------------------------------------------
+struct PlannedPass {
+  DevPass pass;
+  int seg_begin, seg_end;
+};
+
+struct Planner {
+  uint32_t n;
+  int dtype;
+  Geo g;
+  int max_ops = kMaxPassOps;  // ops per pass (the op program lives in shared memory)
+  std::vector<PlannedPass> passes;
+  std::vector<DevSegment> segs;
+  std::vector<DevOp> dops;
+
+  // Choose the ops of one pass from `rem` (indices into ops), program order.
+  // Returns taken indices; fills high mask.
+  std::vector<int> choose(const std::vector<mlb_op_t>& ops, const std::vector<int>& rem, int L,
+                          uint64_t& SH_out) {
+    const uint64_t lowm = (1ull << L) - 1ull;
+    const int Hmax = g.TB - L;
+    const uint64_t allm = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+    // strategy A: first come
+    auto run = [&](uint64_t SH, bool grow, std::vector<int>* taken) {
+      uint64_t blocked = 0;
+      int cnt = 0;
+      for (int idx : rem) {
+        const mlb_op_t& o = ops[idx];
+        const uint64_t Q = op_qubits(o), T = op_targets(o);
+        if (Q & blocked) { blocked |= Q; if (blocked == allm) break; continue; }
+        const uint64_t need = T & ~lowm & ~SH;
+        if (cnt >= max_ops) break;
+        if (need == 0 || (grow && popc(SH | need) <= Hmax)) {
+          SH |= need;
+          cnt++;
+          if (taken) taken->push_back(idx);
+        } else {
+          blocked |= Q;
+          if (blocked == allm) break;
+        }
+      }
+      return std::make_pair(cnt, SH);
+    };
+    auto A = run(0, true, nullptr);
+    // strategy B: the Hmax high qubits most demanded by the first ops
+    std::vector<double> score(n, 0.0);
+    {
+      int seen = 0;
+      for (int idx : rem) {
+        const uint64_t T = op_targets(ops[idx]) & ~lowm;
+        for (uint32_t b = 0; b < n; b++)
+          if (T >> b & 1ull) score[b] += 1.0 / (1.0 + seen * 0.02);
+        if (++seen > 8 * (int)n) break;
+      }
+    }
+    std::vector<int> order;
+    for (uint32_t b = L; b < n; b++) order.push_back((int)b);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return score[a] > score[b]; });
+    uint64_t SHB = 0;
+    for (int k = 0; k < (int)order.size() && k < Hmax; k++)
+      if (score[order[k]] > 0) SHB |= 1ull << order[k];
+    auto B = run(SHB, true, nullptr);
+    std::vector<int> taken;
+    if (B.first > A.first) {
+      run(SHB, true, &taken);
+      SH_out = B.second;
+    } else {
+      run(0, true, &taken);
+      SH_out = A.second;
+    }
+    return taken;
+  }
+
+  // Reorder a pass's ops (list scheduling) so that ops whose targets fit one
+  // register set run back to back: each segment costs a shared-memory round
+  // trip of the whole tile, so fewer, fuller segments are cheaper.  Two ops
+  // commute when neither's non-diagonal targets touch the other's qubits
+  // (controls and diagonal keys commute with each other); an op may only be
+  // scheduled once every earlier op it does not commute with is scheduled.
+  template <typename LocalMask>
+  std::vector<int> schedule_segments(const std::vector<mlb_op_t>& ops, const std::vector<int>& taken,
+                                     LocalMask&& local_mask, int RB) {
+    const size_t N = taken.size();
+    std::vector<uint32_t> T(N), D(N);
+    std::vector<bool> wide(N);
+    for (size_t i = 0; i < N; i++) {
+      const mlb_op_t& o = ops[taken[i]];
+      uint64_t om;
+      local_mask(op_targets(o), T[i], om);
+      local_mask(op_qubits(o) & ~op_targets(o), D[i], om);
+      wide[i] = o.kind == MLB_OP_2Q;
+    }
+    std::vector<int> blockers(N, 0);
+    std::vector<std::vector<int>> after(N);
+    for (size_t i = 0; i < N; i++)
+      for (size_t j = 0; j < i; j++) {
+        const bool commute = (T[i] & (T[j] | D[j])) == 0 && (T[j] & (T[i] | D[i])) == 0;
+        if (!commute) {
+          blockers[i]++;
+          after[j].push_back((int)i);
+        }
+      }
+    std::vector<bool> done(N, false);
+    std::vector<int> out;
+    out.reserve(N);
+    auto take = [&](size_t i) {
+      done[i] = true;
+      out.push_back(taken[i]);
+      for (int k : after[i]) blockers[k]--;
+    };
+    while (out.size() < N) {
+      uint32_t S = 0;
+      bool any = false;
+      bool progress = true;
+      while (progress) {
+        progress = false;
+        for (size_t i = 0; i < N; i++) {
+          if (done[i] || blockers[i] != 0) continue;
+          if (wide[i]) {  // a generic 4x4 op forms its own segment
+            if (!any) {
+              take(i);
+              any = true;
+              progress = false;
+              break;
+            }
+            continue;
+          }
+          if (popc(S | T[i]) <= RB) {
+            S |= T[i];
+            take(i);
+            any = true;
+            progress = true;
+          }
+        }
+        if (any && !out.empty() && ops[out.back()].kind == MLB_OP_2Q) break;
+      }
+    }
+    return out;
+  }
+
+  void lower_pass(const std::vector<mlb_op_t>& ops, const std::vector<int>& taken, int L, uint64_t SH) {
+    PlannedPass pp{};
+    DevPass& P = pp.pass;
+    P.n = (int)n;
+    P.L = L;
+    int local_of[64];
+    for (int q = 0; q < 64; q++) local_of[q] = -1;
+    for (int q = 0; q < L; q++) local_of[q] = q;
+    int H = 0;
+    for (uint32_t q = L; q < n; q++)
+      if (SH >> q & 1ull) {
+        P.high[H] = (int)q;
+        local_of[q] = L + H;
+        H++;
+      }
+    P.H = H;
+    const int m = L + H;
+    const uint64_t allm = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+    P.tile_free_mask = allm & ~(((1ull << L) - 1ull) | SH);
+    P.num_tiles = 1ull << (n - m);
+    const int RB = std::min(g.RB, m);
+    pp.seg_begin = (int)segs.size();
+
+    auto local_mask = [&](uint64_t gm, uint32_t& lm, uint64_t& om) {
+      lm = 0;
+      om = 0;
+      for (uint32_t b = 0; b < n; b++)
+        if (gm >> b & 1ull) {
+          if (local_of[b] >= 0) lm |= 1u << local_of[b];
+          else om |= 1ull << b;
+        }
+    };
+    const std::vector<int> order = schedule_segments(ops, taken, local_mask, RB);
+    const std::vector<int>& taken_in = taken;
+    (void)taken_in;
+    auto run_segments = [&](const std::vector<int>& taken) {
+    size_t i = 0;
+    while (i < taken.size()) {
+      // a generic 4x4 op runs alone in a shared-memory segment
+      if (ops[taken[i]].kind == MLB_OP_2Q) {
+        const mlb_op_t& o = ops[taken[i]];
+        DevSegment sg{};
+        sg.mode = 1;
+        sg.nbits = 0;
+        sg.op_begin = (int)dops.size();
+        DevOp d{};
+        std::memcpy(d.m, o.m, sizeof d.m);
+        local_mask(o.cmask, d.lcmask, d.ocmask);
+        d.kind = DOP_2Q_GEN;
+        d.lt = local_of[o.target];
+        d.k = local_of[o.target2];
+        dops.push_back(d);
+        sg.op_end = (int)dops.size();
+        segs.push_back(sg);
+        i++;
+        continue;
+      }
+      // grow a segment
+      uint32_t bits = 0;
+      size_t j = i;
+      for (; j < taken.size(); j++) {
+        if (ops[taken[j]].kind == MLB_OP_2Q) break;
+        const uint64_t T = op_targets(ops[taken[j]]);
+        uint32_t tl = 0;
+        uint64_t dummy;
+        local_mask(T, tl, dummy);
+        if (popc(bits | tl) > RB) break;
+        bits |= tl;
+      }
+      // pad to RB bits with the lowest free local bits
+      for (int b = 0; b < m && popc(bits) < RB; b++) bits |= 1u << b;
+      DevSegment sg{};
+      sg.nbits = 0;
+      for (int b = 0; b < m; b++)
+        if (bits >> b & 1u) sg.bits[sg.nbits++] = b;
+      auto rpos = [&](int lbit) {
+        for (int k = 0; k < sg.nbits; k++)
+          if (sg.bits[k] == lbit) return k;
+        return -1;
+      };
+      sg.op_begin = (int)dops.size();
+      for (size_t k = i; k < j; k++) {
+        const mlb_op_t& o = ops[taken[k]];
+        DevOp d{};
+        std::memcpy(d.m, o.m, sizeof d.m);
+        local_mask(o.cmask, d.lcmask, d.ocmask);
+        d.lt = -1;
+        switch (o.kind) {
+          case MLB_OP_1Q: {
+            bool real = true;
+            for (int t = 1; t < 8; t += 2)
+              if (o.m[t] != 0.0) real = false;
+            d.kind = real ? DOP_1Q_REAL : DOP_1Q_GEN;
+            d.rt = rpos(local_of[o.target]);
+            break;
+          }
+          case MLB_OP_X: d.kind = DOP_X; d.rt = rpos(local_of[o.target]); break;
+          case MLB_OP_SWAP:
+            d.kind = DOP_SWAP;
+            d.rt = rpos(local_of[o.target]);
+            d.rt2 = rpos(local_of[o.target2]);
+            break;
+          case MLB_OP_DIAG1:
+            d.kind = DOP_DIAG1;
+            d.lt = local_of[o.target];
+            d.omask = d.lt >= 0 ? 0 : (1ull << o.target);
+            break;
+          case MLB_OP_PHASE: {
+            d.kind = DOP_PHASE;
+            local_mask(o.cmask, d.lmask, d.omask);
+            d.lcmask = 0;
+            d.ocmask = 0;
+            break;
+          }
+          case MLB_OP_ZZ: {
+            d.kind = DOP_ZZ;
+            local_mask((1ull << o.target) | (1ull << o.target2), d.lmask, d.omask);
+            break;
+          }
+        }
+        dops.push_back(d);
+      }
+      sg.op_end = (int)dops.size();
+      segs.push_back(sg);
+      i = j;
+    }
+    };
+    run_segments(order);
+    pp.seg_end = (int)segs.size();
+    P.num_segments = pp.seg_end - pp.seg_begin;
+    passes.push_back(pp);
+  }
+
+  void plan(const std::vector<mlb_op_t>& ops) {
+    std::vector<int> rem(ops.size());
+    for (size_t i = 0; i < ops.size(); i++) rem[i] = (int)i;
+    const int L = (int)n <= g.TB ? (int)n : 5;
+    while (!rem.empty()) {
+      uint64_t SH = 0;
+      std::vector<int> taken;
+      if ((int)n <= g.TB) {
+        taken.assign(rem.begin(), rem.begin() + std::min<size_t>(rem.size(), kMaxPassOps));
+      } else {
+        taken = choose(ops, rem, L, SH);
+      }
+      lower_pass(ops, taken, L, SH);
+      // remove taken (both lists ascending)
+      std::vector<int> next;
+      next.reserve(rem.size() - taken.size());
+      size_t t = 0;
+      for (int idx : rem) {
+        if (t < taken.size() && taken[t] == idx) { t++; continue; }
+        next.push_back(idx);
+      }
+      rem.swap(next);
+    }
+  }
+};
+
+
+}  // namespace plan
+}  // namespace mlb

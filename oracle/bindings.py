@@ -330,6 +330,40 @@ def ref_qgtl_execute(n: int, gates, shots: int, seed: int, want_probs: bool = Tr
     return outs, probs
 
 
+class RefSolver:
+    """A vqe_solver_t built through the reference API (HEA ansatz)."""
+
+    def __init__(self, n: int, layers: int, paulis, coeffs, hf_reference: int = 0):
+        L = self.lib = ref()
+        self.h = L.pauli_hamiltonian_create(n, len(paulis))
+        for k, (ps, c) in enumerate(zip(paulis, coeffs)):
+            if L.pauli_hamiltonian_add_term(self.h, float(c), ps.encode(), k):
+                raise RuntimeError("pauli_hamiltonian_add_term")
+        if hf_reference:
+            # pauli_hamiltonian_t.hf_reference (vqe.h:127) sits after
+            # num_qubits, num_terms, terms, nuclear_repulsion, molecule_name,
+            # bond_distance: byte offset 48
+            C.c_uint64.from_address(self.h + 48).value = hf_reference
+        self.ans = L.vqe_create_hardware_efficient_ansatz(n, layers)
+        self.opt = L.vqe_optimizer_create(2)  # any optimizer; vqe_solver_create needs one
+        self.ctx = EntropyCtx(ENTROPY_FN(lambda ud, buf, sz: 0), None)
+        self.solver = L.vqe_solver_create(self.h, self.ans, self.opt, C.byref(self.ctx))
+        self.P = 2 * n * layers
+
+    def gradient(self, params) -> np.ndarray:
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        g = np.empty(self.P, dtype=np.float64)
+        rc = self.lib.moonlab_vqe_gradient(self.solver, _dp(p), _dp(g), self.P)
+        if rc:
+            raise RuntimeError(f"moonlab_vqe_gradient: {rc}")
+        return g
+
+    def close(self):
+        if self.solver:
+            self.lib.vqe_solver_free(self.solver)
+            self.solver = None
+
+
 def ref_vqe_gradient(n: int, layers: int, paulis, coeffs, params) -> np.ndarray:
     """moonlab_vqe_gradient on a HEA solver built through the reference API."""
     L = ref()

@@ -119,3 +119,16 @@ def test_planner_small_state_single_tile():
     assert st.passes == -(-st.ops // 160)
     st = plan(brickwork(10, 5, 7), 10)
     assert st.passes == 1
+
+
+def test_adjoint_problem_needs_a_device_and_valid_terms():
+    lib = _lib.load()
+    h = C.c_void_p()
+    x = (C.c_uint64 * 1)(1 << 9)
+    z = (C.c_uint64 * 1)(0)
+    c = (C.c_double * 1)(1.0)
+    # term outside a 4-qubit register is rejected before any device work
+    assert lib.mlb_hea_create(4, 2, 0, 1, x, z, c, 0, 0, C.byref(h)) == -4
+    if not _has_gpu():
+        x[0] = 1
+        assert lib.mlb_hea_create(4, 2, 0, 1, x, z, c, 0, 0, C.byref(h)) == -2
