@@ -360,7 +360,8 @@ int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, do
   if ((rc = grow(h->d_epart, h->epart_cap, max_tiles))) return rc;
   if ((rc = grow(h->d_out, h->out_cap, B + B * h->P))) return rc;
   // 2. forward
-  if ((rc = launch_adj_init(h->dtype, h->psi, (int)h->n, B, h->hf, h->stream))) return hfail(rc, "init kernel");
+  // |0...0>: the tape itself starts with X on the hf_reference bits (vqe.c:1953-1959)
+  if ((rc = launch_adj_init(h->dtype, h->psi, (int)h->n, B, 0, h->stream))) return hfail(rc, "init kernel");
   for (auto& gp : h->fwd) {
     AdjPass P = gp.P;
     P.num_tiles = P.tiles_per_state * B;

@@ -167,8 +167,12 @@ __global__ void __launch_bounds__(AdjCfg<Real>::NT, 2)
 #pragma unroll
       for (int q = 0; q < kRB; q++) bm[q] = 1u << seg.bits[q];
       const uint32_t groups = amps >> kRB;
-      for (uint32_t gi = threadIdx.x; gi < groups; gi += NT) {
-        uint32_t gb = gi;
+      // Every lane runs every iteration (the gradient partials use full-warp
+      // shuffles); lanes past the last group work on zeros and store nothing.
+      for (uint32_t g0 = 0; g0 < groups; g0 += NT) {
+        const uint32_t gi = g0 + threadIdx.x;
+        const bool active = gi < groups;
+        uint32_t gb = active ? gi : 0u;
 #pragma unroll
         for (int q = 0; q < kRB; q++) {
           const uint32_t p = seg.bits[q];
@@ -181,8 +185,8 @@ __global__ void __launch_bounds__(AdjCfg<Real>::NT, 2)
 #pragma unroll
           for (int q = 0; q < kRB; q++)
             if (k >> q & 1) loc |= bm[q];
-          v[k] = sv[aswz<Real>(loc)];
-          if (DUAL) w[k] = sw[aswz<Real>(loc)];
+          v[k] = active ? sv[aswz<Real>(loc)] : A{0, 0};
+          if (DUAL) w[k] = active ? sw[aswz<Real>(loc)] : A{0, 0};
         }
         for (int o = seg.op_begin; o < seg.op_end; o++) {
           if (!son[o]) continue;
@@ -228,14 +232,16 @@ __global__ void __launch_bounds__(AdjCfg<Real>::NT, 2)
             }
           }
         }
+        if (active) {
 #pragma unroll
-        for (int k = 0; k < kG; k++) {
-          uint32_t loc = gb;
+          for (int k = 0; k < kG; k++) {
+            uint32_t loc = gb;
 #pragma unroll
-          for (int q = 0; q < kRB; q++)
-            if (k >> q & 1) loc |= bm[q];
-          sv[aswz<Real>(loc)] = v[k];
-          if (DUAL) sw[aswz<Real>(loc)] = w[k];
+            for (int q = 0; q < kRB; q++)
+              if (k >> q & 1) loc |= bm[q];
+            sv[aswz<Real>(loc)] = v[k];
+            if (DUAL) sw[aswz<Real>(loc)] = w[k];
+          }
         }
       }
       __syncthreads();
@@ -351,12 +357,10 @@ int launch_gates_t(void* psi, void* lam, const AdjPass& P, const AdjOp* d_ops, c
   using A = typename Cplx<Real>::T;
   const size_t smem = sizeof(A) * ((size_t)(dual ? 2 : 1) << (P.L + P.H));
   auto launch = [&](auto kern) {
-    static bool set = false;
-    if (!set) {
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(2 * sizeof(A) << AdjCfg<Real>::TB));
-      set = true;
-    }
+    // Every instantiation has the same pointer type, so the opt-in is set per
+    // launch (an idempotent attribute write) rather than once per type.
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(2 * sizeof(A) << AdjCfg<Real>::TB));
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, AdjCfg<Real>::NT, smem);
     uint64_t grid = (uint64_t)num_sms * (per_sm < 1 ? 1 : per_sm);
