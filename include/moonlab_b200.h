@@ -125,6 +125,33 @@ int  mlb_correlation_zz(mlb_state_t *s, uint32_t q1, uint32_t q2, double *out);
 int  mlb_expect_pauli(mlb_state_t *s, uint64_t xmask, uint64_t zmask, double *out);
 int  mlb_expect_pauli_sum(mlb_state_t *s, size_t num_terms, const uint64_t *xmasks,
                           const uint64_t *zmasks, const double *coeffs, double *out);
+/* mlb_prob_one_all_noalloc: the one-pass reduction of mlb_prob_one_all and
+ * mlb_norm_sq, run on amplitudes the caller owns and written to device
+ * memory the caller owns.  It allocates nothing.  No counterpart in the
+ * reference (its reductions read host memory).
+ *   amp_device  2^num_qubits amplitudes of `dtype` (MLB_C128 / MLB_C64) in
+ *               memory of the current device;
+ *   out_device  num_qubits + 1 doubles on the same device: P(qubit q = 1)
+ *               for q < num_qubits, then the squared norm;
+ *   stream      a cudaStream_t of the current device (NULL: default stream).
+ *               The call only enqueues two kernels; out_device is ready when
+ *               the stream has run them.
+ * Meant for callers that may not allocate device memory: a process that has
+ * reserved all of HBM up front under a fixed budget (a serving process, or a
+ * host framework whose own allocator owns the device), and latency-critical
+ * loops where cudaMalloc / cudaFree would stall on device synchronisation.
+ * Its scratch is one fixed array per device inside this library, 1,163,264
+ * bytes, which sets the limit: num_qubits 1..30, else MLB_ERR_NUM_QUBITS.
+ * All calls on a device share that array: two calls whose kernels overlap on
+ * the GPU (different streams, or different host threads) race and return
+ * wrong values, so order them on one stream or synchronise between them.
+ * Each call writes every scratch entry it reads; nothing needs clearing.
+ * The first call on a device does a one-time set-up (it looks up the
+ * array's address and the SM count); make that first call before any stream
+ * capture on that device.  Errors: MLB_ERR_INVALID_ARG for null, misaligned
+ * or non-device buffers and a bad dtype. */
+int  mlb_prob_one_all_noalloc(const void *amp_device, int dtype, uint32_t num_qubits,
+                              double *out_device, void *stream);
 /* probability vector; rule 0 = cabs(a)^2 (measurement.c:140),
  * rule 1 = re*re + im*im (moonlab_qgtl_backend.c:199-210).
  * out_host may be NULL when out_device is given (device pointer, 2^n doubles). */

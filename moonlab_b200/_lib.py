@@ -88,6 +88,7 @@ _SIGS = {
     "mlb_norm_sq": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "mlb_prob_one": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)]),
     "mlb_prob_one_all": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "mlb_prob_one_all_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p]),
     "mlb_expect_z_all": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "mlb_prob_one_exact": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)]),
     "mlb_correlation_zz": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_double)]),

@@ -76,6 +76,8 @@ struct DeviceGuard {
 
 }  // namespace
 
+int mlb::record_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 struct mlb_state {
   uint32_t n = 0;
   int dtype = MLB_C128;

@@ -9,6 +9,10 @@
 // Per amplitude that costs one |a|^2 and ~2.5 FP64 adds; the chunk totals go
 // to a small buffer that a second kernel folds into the high-bit sums.
 // All reductions use a fixed order, so results are identical run to run.
+#include <algorithm>
+#include <atomic>
+#include <mutex>
+
 #include "kernels_common.cuh"
 #include "hypot_glibc.cuh"
 #include "mlb_internal.h"
@@ -302,3 +306,100 @@ int launch_scale(int dtype, void* amp, int n, double factor, uint64_t keep_mask,
 }
 
 }  // namespace mlb
+
+// ---- probs_z without device allocation -------------------------------------
+// mlb_prob_one_all_noalloc runs the probs_z reduction above on caller-owned
+// buffers, with its scratch in one fixed array per device instead of a
+// cudaMalloc'd buffer.  Scratch use: pass-1 partials ([grid x 14] doubles,
+// grid <= kNoAllocMaxParts) followed by one total per 2^13-amplitude chunk
+// (2^(n-13) doubles, at most 2^17 for n = 30).  Pass 1 writes every entry
+// pass 2 reads, so nothing is cleared between calls.
+namespace {
+
+constexpr uint32_t kNoAllocMaxQubits = 30;
+constexpr int kNoAllocMaxParts = 1024;  // pass-1 CTAs; the grid is min(chunks, 4 * SMs)
+constexpr size_t kNoAllocScratchDoubles =
+    (size_t)kNoAllocMaxParts * (1 + 13) + (size_t(1) << (kNoAllocMaxQubits - 13));  // 145,408
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_probs_z_scratch[kNoAllocScratchDoubles];
+
+struct NoAllocDevice {
+  std::atomic<double*> scratch{nullptr};
+  int num_sms = 0;
+};
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+// Set-up, once per device, with that device current: the array's address and
+// the SM count.
+int noalloc_setup(int dev, double** scratch, int* num_sms) {
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  double* p = d.scratch.load(std::memory_order_acquire);
+  if (!p) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    p = d.scratch.load(std::memory_order_relaxed);
+    if (!p) {
+      int sms = 0;
+      cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess || sms <= 0)
+        return mlb::record_error(MLB_ERR_DRIVER, "mlb_prob_one_all_noalloc: SM count query failed");
+      void* addr = nullptr;
+      e = cudaGetSymbolAddress(&addr, g_probs_z_scratch);
+      if (e != cudaSuccess || !addr)
+        return mlb::record_error(MLB_ERR_DRIVER, "mlb_prob_one_all_noalloc: scratch address lookup failed");
+      d.num_sms = sms;
+      p = (double*)addr;
+      d.scratch.store(p, std::memory_order_release);
+    }
+  }
+  *scratch = p;
+  *num_sms = d.num_sms;
+  return MLB_OK;
+}
+
+// True when ptr is device (or managed) memory of device dev.
+bool on_device(const void* ptr, int dev) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev;
+}
+
+}  // namespace
+
+extern "C" int mlb_prob_one_all_noalloc(const void* amp_device, int dtype, uint32_t num_qubits,
+                                        double* out_device, void* stream) {
+  if (!amp_device || !out_device)
+    return mlb::record_error(MLB_ERR_INVALID_ARG, "mlb_prob_one_all_noalloc: null buffer");
+  if (dtype != MLB_C128 && dtype != MLB_C64)
+    return mlb::record_error(MLB_ERR_INVALID_ARG, "mlb_prob_one_all_noalloc: dtype must be MLB_C128 or MLB_C64");
+  if (num_qubits < 1 || num_qubits > kNoAllocMaxQubits)
+    return mlb::record_error(MLB_ERR_NUM_QUBITS,
+                             "mlb_prob_one_all_noalloc: num_qubits must be 1..30 (fixed scratch size)");
+  const uintptr_t align = dtype == MLB_C128 ? 16 : 8;
+  if ((uintptr_t)amp_device % align || (uintptr_t)out_device % 8)
+    return mlb::record_error(MLB_ERR_INVALID_ARG, "mlb_prob_one_all_noalloc: misaligned buffer");
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return mlb::record_error(MLB_ERR_NO_DEVICE, "mlb_prob_one_all_noalloc: no current device");
+  }
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return mlb::record_error(MLB_ERR_NOT_SUPPORTED, "mlb_prob_one_all_noalloc: device ordinal above 63");
+  if (!on_device(amp_device, dev) || !on_device(out_device, dev))
+    return mlb::record_error(MLB_ERR_INVALID_ARG,
+                             "mlb_prob_one_all_noalloc: buffers must be device memory of the current device");
+  double* scratch = nullptr;
+  int num_sms = 0;
+  int rc = noalloc_setup(dev, &scratch, &num_sms);
+  if (rc) return rc;
+  // grid = min(chunks, 4 * SMs) stays within the array's kNoAllocMaxParts CTAs.
+  const int sms = std::min(num_sms, kNoAllocMaxParts / 4);
+  rc = mlb::launch_reduce_probs_z(dtype, amp_device, (int)num_qubits, out_device, scratch, sms,
+                                  (cudaStream_t)stream);
+  if (rc) return mlb::record_error(rc, "mlb_prob_one_all_noalloc: launch failed");
+  return MLB_OK;
+}

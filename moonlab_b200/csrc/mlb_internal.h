@@ -147,4 +147,7 @@ int seq_sum_exact(int dtype, const void* amp, int n, uint64_t fmask, uint64_t fv
 uint64_t kernel_launch_count();
 void count_launch(uint64_t k = 1);
 
+// Records the message mlb_last_error() returns on this thread; returns code.
+int record_error(int code, const char* msg);
+
 }  // namespace mlb
