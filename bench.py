@@ -49,6 +49,20 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def profiled_traffic(n: int):
+    """DRAM bytes of one k_tile<double> pass at n qubits: the ncu figure of
+    bytes per amplitude (profiles/k_tile_c128_26q.md, dram read + write of
+    a 26-qubit pass) times 2^n.  A pass moves every amplitude once each way,
+    so its traffic grows in proportion to 2^n.  None if the summary is gone."""
+    p = ROOT / "profiles" / "k_tile_c128_26q.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_amplitude_per_pass:"):
+            return float(line.split(":")[1]) * (1 << n)
+    return None
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle samples during the timed region."""
 
@@ -322,8 +336,9 @@ def run_b200(args, ws, rank, local):
                        "tile_passes_per_circuit": passes, "gates": int(len(gates))},
             "hbm_gbs_per_pass": achieved,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "k_tile<double>",
-                         "peak_source": peak_kind},
+                         "frac": achieved / peak, "traffic": profiled_traffic(n),
+                         "kernel": "k_tile<double>", "peak_source": peak_kind,
+                         "algorithmic_bytes_per_pass": per_pass_bytes},
             "c64": {"circuit_ms": c64_s * 1e3, "speedup_vs_c128": t_max / c64_s, "fidelity": fid,
                     "max_amp_err": maxerr, "path": "c64 tiled"},
             "e2e": {"value": ws / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": int(h2d),
