@@ -194,6 +194,37 @@ int  mlb_gates_to_ops(const mlb_gate_t *gates, size_t num_gates, uint32_t num_qu
                       mlb_op_t *ops_out, size_t *num_ops_out);
 int  mlb_run_gates(mlb_state_t *s, const mlb_gate_t *gates, size_t num_gates);
 
+/* ---- scheduler jobs -------------------------------------------------------
+ * A job as the reference's scheduler holds it (src/distributed/scheduler.c:
+ * num_qubits, gate records of the QGTL enum, total shots, worker fan-out,
+ * base seed).  mlb_job_parse_json reads the text of moonlab_job_to_json
+ * (scheduler.c:492-537; theta printed with %.17g, so it round-trips
+ * exactly).  Pass gates = NULL to learn the gate count; with a buffer that
+ * is too small the call returns MLB_ERR_INVALID_ARG and sets *num_gates to
+ * the count needed.  Malformed text: MLB_ERR_INVALID_ARG. */
+typedef struct {
+    int32_t  num_qubits;
+    int32_t  num_shots;
+    int32_t  num_workers;
+    int32_t  reserved;
+    uint64_t rng_seed;
+} mlb_job_desc_t;
+int  mlb_job_parse_json(const char *json, mlb_job_desc_t *desc, mlb_gate_t *gates,
+                        size_t capacity, size_t *num_gates);
+/* Run a job with the semantics of the scheduler's default "simulator"
+ * backend (simulator_backend_execute, scheduler.c:194-239): workers =
+ * min(num_workers, num_shots), worker w takes shots [w S / W, (w+1) S / W)
+ * and draws its uniforms from xorshift64 seeded with
+ * splitmix64(rng_seed ^ (w << 32)) (moonlab_qgtl_backend.c:158-167,
+ * :226-240); each shot is measurement_all_qubits on the circuit's output
+ * state.  Here the circuit runs once, on `device`, in complex128, and all
+ * shots are sampled from that state; outcomes[num_shots] are bit-identical
+ * to the reference's for a non-zero rng_seed (a zero seed takes the clock,
+ * as the reference does).  *workers_used and *seconds (wall time of the
+ * whole job) may be NULL. */
+int  mlb_job_run(const mlb_job_desc_t *desc, const mlb_gate_t *gates, size_t num_gates,
+                 int device, uint64_t *outcomes, int *workers_used, double *seconds);
+
 /* Plan statistics of the last flush: passes launched and ops applied. */
 typedef struct {
     uint64_t passes;

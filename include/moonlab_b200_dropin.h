@@ -109,6 +109,30 @@ int moonlab_vqe_gradient(void *solver, const double *parameters, double *gradien
 int moonlab_b200_vqe_gradient_batch(void *solver, size_t batch, const double *parameters,
                                     double *gradients_out, size_t num_parameters);
 
+/* ---- scheduler backend plug-in (src/distributed/scheduler.h:225-262,
+ *      registry scheduler.c:283-305).
+ * moonlab_b200_backend_execute is a moonlab_backend_execute_fn: it reads the
+ * job through the reference's moonlab_job_to_json, runs it on the B200 with
+ * the "simulator" backend's semantics (mlb_job_run) and fills the
+ * moonlab_job_results_t the scheduler passes in (outcomes and
+ * worker_seconds malloc'ed, freed by the scheduler).  Returns
+ * MOONLAB_SCHED_OK (0), MOONLAB_SCHED_BAD_ARG (-501), MOONLAB_SCHED_OOM
+ * (-502) or MOONLAB_SCHED_INTERNAL (-503).  ctx: NULL (device 0) or a
+ * pointer to an int device ordinal.
+ * moonlab_b200_register_backend registers it under the name "b200" with the
+ * scheduler loaded in the process (found with dlsym, so this library does
+ * not link against the reference); after it, moonlab_job_set_backend(job,
+ * "b200") routes moonlab_scheduler_run to the GPU.  Returns the registry's
+ * code, or MOONLAB_SCHED_BACKEND_NOT_FOUND (-506) when no scheduler is
+ * loaded.  A host that opened the reference library privately (RTLD_LOCAL,
+ * as ctypes does by default) passes its moonlab_register_backend and
+ * moonlab_job_to_json to moonlab_b200_register_backend_with instead.
+ * moonlab_b200_release_backend_state frees the cached device state. */
+int moonlab_b200_backend_execute(const void *job, void *results, void *ctx);
+int moonlab_b200_register_backend(void);
+int moonlab_b200_register_backend_with(void *register_fn, void *job_to_json_fn);
+void moonlab_b200_release_backend_state(void);
+
 /* The engine handle behind a GPU-backed quantum_state_t (for callers that
  * want the engine's FP64 reductions, sampling and collapse directly). */
 struct mlb_state *moonlab_b200_engine_of(quantum_state_t *state);

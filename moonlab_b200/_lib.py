@@ -43,6 +43,11 @@ class MlbFlushStats(C.Structure):
                 ("gpu_ms", C.c_double)]
 
 
+class MlbJobDesc(C.Structure):
+    _fields_ = [("num_qubits", C.c_int32), ("num_shots", C.c_int32), ("num_workers", C.c_int32),
+                ("reserved", C.c_int32), ("rng_seed", C.c_uint64)]
+
+
 class QuantumState(C.Structure):
     """quantum_state_t (reference src/quantum/state.h:102-131)."""
     _fields_ = [("num_qubits", C.c_size_t), ("state_dim", C.c_size_t), ("amplitudes", C.c_void_p),
@@ -125,6 +130,14 @@ _SIGS = {
     "moonlab_vqe_gradient": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_size_t]),
     "moonlab_b200_vqe_gradient_batch": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), C.c_size_t]),
+    "mlb_job_parse_json": (C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                     C.POINTER(C.c_size_t)]),
+    "mlb_job_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.POINTER(C.c_uint64),
+                              C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "moonlab_b200_backend_execute": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "moonlab_b200_register_backend": (C.c_int, []),
+    "moonlab_b200_register_backend_with": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "moonlab_b200_release_backend_state": (None, []),
     "mlb_status_string": (C.c_char_p, [C.c_int]),
     "mlb_last_error": (C.c_char_p, []),
     # reference-compatible drop-in surface
