@@ -316,6 +316,8 @@ def run_b200(args, ws, rank, local):
     fid = float(ip.abs().item() ** 2)
     s64.close()
 
+    serving = None if args.no_serving else serving_leg(args, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -347,8 +349,37 @@ def run_b200(args, ws, rank, local):
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
+        if serving is not None:
+            line["serving"] = serving
         print(json.dumps(line), flush=True)
     sv.close()
+
+
+def serving_leg(args, local):
+    """The request stream (Poisson arrivals; qubits U{10..28}, depth
+    U{10..100}, shots U{1..4096}, dtype 50/50) on this rank's GPU through
+    the continuous-batching server: first all requests at once (capacity,
+    circuits/s), then paced at --serve-rate (latency p50/p99 at that load).
+    Latency = submit to result on the host clock; circuits/s = requests /
+    (last result - first submit)."""
+    from moonlab_b200.circuits import config_c5
+    from moonlab_b200.serving import Server, request_circuit, run_load
+    reqs = config_c5(num=args.serve_requests, rate=args.serve_rate)
+    circ = [request_circuit(r) for r in reqs]
+    workers = 8
+    with Server(device=local, workers=workers) as srv:
+        sat = run_load(srv, reqs, time_scale=0.0, circuits=circ)
+        paced = run_load(srv, reqs, time_scale=1.0, circuits=circ)
+    return {
+        "workload": (f"{len(reqs)} requests of the Poisson stream (seed 0xC5): qubits U{{10..28}}, "
+                     "depth U{10..100} brickwork, shots U{1..4096}, c128/c64 50/50"),
+        "rate_per_s": args.serve_rate, "workers": workers,
+        "circuits_per_s": paced["circuits_per_s"], "p50_ms": paced["p50_s"] * 1e3,
+        "p99_ms": paced["p99_s"] * 1e3, "mean_ms": paced["mean_s"] * 1e3,
+        "saturated_circuits_per_s": sat["circuits_per_s"], "saturated_p99_ms": sat["p99_s"] * 1e3,
+        "peak_running": paced["stats"]["peak_running"],
+        "peak_reserved_gib": paced["stats"]["peak_reserved_bytes"] / 2**30,
+    }
 
 
 class _DeviceView:
@@ -369,6 +400,9 @@ def main():
     ap.add_argument("--depth", type=int, default=40)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-rate", type=float, default=15.0)
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     try:

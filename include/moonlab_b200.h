@@ -225,6 +225,52 @@ int  mlb_job_parse_json(const char *json, mlb_job_desc_t *desc, mlb_gate_t *gate
 int  mlb_job_run(const mlb_job_desc_t *desc, const mlb_gate_t *gates, size_t num_gates,
                  int device, uint64_t *outcomes, int *workers_used, double *seconds);
 
+/* ---- serving: a continuous-batching request loop on one GPU --------------
+ * mlb_server_submit queues a request and returns at once with a ticket.
+ * num_workers threads admit queued requests in arrival order whenever a
+ * worker and HBM budget are free (first fit; a request waiting longer than
+ * 0.5 s holds back later ones), so requests that arrive while others run
+ * start without waiting for a batch to finish and overlap on the device.
+ * Device states are pooled per (qubits, dtype) and count against the
+ * budget (0 = 80 % of the device's free memory at creation).  A request's
+ * shots follow moonlab_qgtl_execute (moonlab_qgtl_backend.c:218-240):
+ * uniforms from xorshift64(rng_seed), each shot measurement_all_qubits(u) on
+ * the circuit's output state (rng_seed 0 takes the clock).  Results do not
+ * depend on the other requests in flight.  Times in mlb_request_info_t are
+ * seconds since the server was created.  mlb_server_wait blocks up to
+ * timeout_ms (< 0: no limit; MLB_ERR_TIMEOUT when it runs out), copies the
+ * outcomes (capacity >= num_shots), releases the ticket and returns the
+ * request's status.  mlb_server_destroy cancels requests not yet admitted
+ * (MLB_ERR_BUSY), lets running ones finish and frees everything; no thread
+ * may be inside mlb_server_wait when it is called. */
+typedef struct mlb_server mlb_server_t;
+typedef struct {
+    uint32_t          num_qubits;
+    int32_t           dtype;        /* MLB_C128 or MLB_C64 */
+    const mlb_gate_t *gates;        /* copied at submit */
+    size_t            num_gates;
+    uint32_t          num_shots;
+    uint32_t          reserved;
+    uint64_t          rng_seed;
+} mlb_request_t;
+typedef struct {
+    int32_t  status;
+    uint32_t num_qubits;
+    int32_t  dtype;
+    uint32_t num_shots;
+    double   submit_s, admit_s, done_s;
+} mlb_request_info_t;
+typedef struct {
+    uint64_t submitted, completed, failed, pending, running, peak_running;
+    uint64_t reserved_bytes, peak_reserved_bytes, budget_bytes;
+} mlb_server_stats_t;
+int  mlb_server_create(int device, size_t hbm_budget_bytes, int num_workers, mlb_server_t **out);
+int  mlb_server_submit(mlb_server_t *s, const mlb_request_t *req, uint64_t *ticket);
+int  mlb_server_wait(mlb_server_t *s, uint64_t ticket, int timeout_ms, uint64_t *outcomes,
+                     size_t capacity, mlb_request_info_t *info);
+int  mlb_server_get_stats(mlb_server_t *s, mlb_server_stats_t *out);
+void mlb_server_destroy(mlb_server_t *s);
+
 /* Plan statistics of the last flush: passes launched and ops applied. */
 typedef struct {
     uint64_t passes;

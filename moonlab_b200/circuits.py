@@ -44,7 +44,15 @@ class SplitMix64:
         return (self.next() >> 11) * (1.0 / 9007199254740992.0)
 
     def uniforms(self, k: int) -> np.ndarray:
-        return np.array([self.uniform() for _ in range(k)], dtype=np.float64)
+        """The next k uniform() values at once (same sequence)."""
+        if k <= 0:
+            return np.empty(0, dtype=np.float64)
+        z = np.uint64(self.state) + np.arange(1, k + 1, dtype=np.uint64) * np.uint64(GAMMA)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+        self.state = (self.state + k * GAMMA) & MASK64
+        return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
     def gauss(self) -> float:
         u1 = self.uniform()
@@ -65,21 +73,36 @@ def brickwork(n: int, depth: int, seed: int, zz_every: int = 0) -> np.ndarray:
     """Random brickwork circuit: per layer RX, RY, RZ on every qubit with
     angles U[0, 2pi), then CNOT(q, q+1) for q = (layer mod 2), step 2.  With
     zz_every = k > 0, after every layer l with (l + 1) mod k == 0 a ZZ(theta)
-    on every neighbour pair (q, q+1), theta ~ U[0, 2pi)."""
-    rng = SplitMix64(seed)
-    gates = []
+    on every neighbour pair (q, q+1), theta ~ U[0, 2pi).  Angles are drawn
+    from SplitMix64(seed) in gate order."""
+    zz_layers = [l for l in range(depth) if zz_every and (l + 1) % zz_every == 0]
+    u = SplitMix64(seed).uniforms(3 * n * depth + len(zz_layers) * max(n - 1, 0))
+    layers = []
+    pos = 0
+    qs = np.arange(n, dtype=np.int32)
     for layer in range(depth):
-        for q in range(n):
-            for gt in (GATE_RX, GATE_RY, GATE_RZ):
-                gates.append((gt, q, -1, 0, 2.0 * math.pi * rng.uniform()))
-        q = layer % 2
-        while q + 1 < n:
-            gates.append((GATE_CNOT, q + 1, q, 0, 0.0))  # control q, target q+1
-            q += 2
-        if zz_every and (layer + 1) % zz_every == 0:
-            for q in range(n - 1):
-                gates.append((GATE_ZZ, q + 1, q, 0, 2.0 * math.pi * rng.uniform()))
-    return np.array(gates, dtype=GATE_DTYPE)
+        rot = np.zeros(3 * n, dtype=GATE_DTYPE)
+        rot["type"] = np.tile(np.array([GATE_RX, GATE_RY, GATE_RZ], dtype=np.int32), n)
+        rot["target"] = np.repeat(qs, 3)
+        rot["control"] = -1
+        rot["theta"] = 2.0 * math.pi * u[pos:pos + 3 * n]
+        pos += 3 * n
+        layers.append(rot)
+        c = np.arange(layer % 2, n - 1, 2, dtype=np.int32)
+        cx = np.zeros(len(c), dtype=GATE_DTYPE)
+        cx["type"] = GATE_CNOT
+        cx["target"] = c + 1  # control q, target q+1
+        cx["control"] = c
+        layers.append(cx)
+        if zz_every and (layer + 1) % zz_every == 0 and n > 1:
+            zz = np.zeros(n - 1, dtype=GATE_DTYPE)
+            zz["type"] = GATE_ZZ
+            zz["target"] = qs[1:]
+            zz["control"] = qs[:-1]
+            zz["theta"] = 2.0 * math.pi * u[pos:pos + n - 1]
+            pos += n - 1
+            layers.append(zz)
+    return np.concatenate(layers) if layers else np.zeros(0, dtype=GATE_DTYPE)
 
 
 def config_c1(n: int = 20, depth: int = 20):

@@ -18,6 +18,7 @@
 // masks and diagonal keys on qubits outside the tile -- is evaluated once
 // per tile.  Shared memory is XOR-swizzled on 128-byte rows so that group
 // gathers of any stride are bank-conflict free.
+#include <atomic>
 #include <cstdio>
 
 #include "kernels_common.cuh"
@@ -370,11 +371,16 @@ int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, cons
   using A = typename Cplx<Real>::T;
   constexpr int NT = TileCfg<Real>::NT;
   const size_t smem = sizeof(A) << (pass.L + pass.H);
-  static bool attr_set = false;
+  // The shared-memory opt-in is a per-device function attribute; set it once
+  // per device (threads may race here, and setting it twice is harmless).
+  static std::atomic<uint64_t> attr_set_mask{0};
   const size_t max_smem = sizeof(A) << TileCfg<Real>::TB;
-  if (!attr_set) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(attr_set_mask.load(std::memory_order_acquire) & bit)) {
     cudaFuncSetAttribute(k_tile<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
-    attr_set = true;
+    attr_set_mask.fetch_or(bit, std::memory_order_release);
   }
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<Real>, NT, smem);

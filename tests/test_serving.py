@@ -1,0 +1,102 @@
+"""The continuous-batching request loop (mlb_server_*).
+
+Each request's outcomes are the same alone and in a concurrent mix (both
+dtypes, bit-identical), complex128 outcomes equal the oracle's
+moonlab_qgtl_execute restatement (pinned to the reference), requests that
+arrive while a large one runs are admitted and finish before it, admission
+holds the HBM budget, and the error paths report what they should."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from moonlab_b200 import _lib
+from moonlab_b200.circuits import Request, brickwork, config_c5
+from oracle import bindings as B
+
+
+def test_request_stream_is_seeded():
+    a, b = config_c5(num=50), config_c5(num=50)
+    assert a == b
+    assert all(10 <= r.n <= 28 and 10 <= r.depth <= 100 and 1 <= r.shots <= 4096 for r in a)
+    assert all(x.arrival < y.arrival for x, y in zip(a, a[1:]))
+
+
+def test_server_needs_a_device():
+    from moonlab_b200.serving import _bind
+    lib = _bind()
+    cnt = C.c_int()
+    if lib.mlb_device_count(C.byref(cnt)) == 0 and cnt.value > 0:
+        pytest.skip("a device is present")
+    h = C.c_void_p()
+    assert lib.mlb_server_create(0, 0, 4, C.byref(h)) == -2
+
+
+def _mix(num, seed=0x5E):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(num):
+        n = int(rng.integers(10, 21))
+        reqs.append(Request(i, 0.0, n, int(rng.integers(5, 30)), int(rng.integers(1, 600)),
+                            int(rng.integers(0, 2)), int(rng.integers(1, 2**63))))
+    return reqs
+
+
+@pytest.mark.gpu
+def test_same_alone_and_in_the_mix(gpu):
+    from moonlab_b200.serving import Server, request_circuit
+    reqs = _mix(40)
+    circ = [request_circuit(r) for r in reqs]
+    alone = []
+    with Server(workers=1) as s:
+        for r, g in zip(reqs, circ):
+            t = s.submit(r.n, g, r.shots, r.seed, "c64" if r.dtype else "c128")
+            alone.append(s.wait(t)[0])
+    # all at once, 8 in flight, a budget that holds only a few 20-qubit states
+    with Server(workers=8, hbm_budget=(16 << 20) * 4 + (8 << 20)) as s:
+        tickets = [s.submit(r.n, g, r.shots, r.seed, "c64" if r.dtype else "c128") for r, g in zip(reqs, circ)]
+        mixed = [s.wait(t)[0] for t in tickets]
+        st = s.stats()
+    assert st["peak_running"] > 1
+    assert st["peak_reserved_bytes"] <= st["budget_bytes"]
+    for a, b in zip(alone, mixed):
+        assert np.array_equal(a, b)
+    # complex128 against the oracle's moonlab_qgtl_execute (bit-exact)
+    for r, g, out in zip(reqs, circ, mixed):
+        if r.dtype == 0 and r.n <= 16:
+            want = np.empty(r.shots, dtype=np.uint64)
+            sv = B.to_svo(g)
+            assert B.port().svo_qgtl_execute(r.n, sv, len(sv), r.shots, r.seed,
+                                              want.ctypes.data_as(C.POINTER(C.c_uint64)), None) == 0
+            assert np.array_equal(out, want)
+
+
+@pytest.mark.gpu
+def test_late_arrivals_overtake_a_long_request(gpu):
+    from moonlab_b200.serving import Server
+    with Server(workers=4) as s:
+        big = s.submit(27, brickwork(27, 80, 1), 16, 7, "c128")
+        small = [s.submit(12, brickwork(12, 10, 2 + i), 64, 9 + i, "c64") for i in range(6)]
+        infos = [s.wait(t)[1] for t in small]
+        _, binfo = s.wait(big)
+    assert all(i["admit_s"] < binfo["done_s"] for i in infos)
+    assert all(i["done_s"] < binfo["done_s"] for i in infos)
+
+
+@pytest.mark.gpu
+def test_budget_errors_and_timeouts(gpu):
+    from moonlab_b200.serving import Server
+    from moonlab_b200._lib import MlbError
+    with Server(workers=1, hbm_budget=64 << 20) as s:
+        with pytest.raises(MlbError):
+            s.submit(26, brickwork(26, 1, 3), 1, 1)  # 1 GiB state > 64 MiB budget
+        t1 = s.submit(20, brickwork(20, 60, 4), 1, 1)
+        t2 = s.submit(20, brickwork(20, 60, 5), 1, 1)
+        with pytest.raises(TimeoutError):
+            s.wait(t2, timeout_ms=0)  # behind t1 on the single worker
+        s.wait(t1)
+        out, info = s.wait(t2)
+        assert info["status"] == 0 and len(out) == 1
+        assert s.stats()["completed"] == 2
