@@ -289,6 +289,31 @@ int  mlb_state_set_timing(mlb_state_t *s, int enable);
  * reports the passes and algorithmic bytes a flush of these ops launches. */
 int  mlb_plan_ops(const mlb_op_t *ops, size_t num_ops, uint32_t num_qubits, int dtype,
                   int fuse1q, mlb_flush_stats_t *out);
+/* The fused complex64 path's plan for these ops, as a flush in MLB_EXEC_FUSED
+ * mode would launch it (host only).  Passes: tile = qubits 0..4 plus
+ * hbits[0..7] (tile bit 5 + i <-> hbits[i]); blocks
+ * [block_begin, block_begin + num_blocks) act on every tile in order.  A
+ * block acts on tile bits pos[0..4] (block index bit j <-> pos[j]); rows
+ * lists the other 8 tile bits.  Its operand image (16 KiB at image * 16384)
+ * holds U' = [Re U -Im U; Im U Re U] as bf16 hi (first 8 KiB) and lo
+ * (U' - hi) in the tensor core's K-major 128-byte-swizzled layout: element
+ * (n, k) at byte (n / 8) * 1024 + (n % 8) * 128 + 2 k with the 16-byte
+ * chunk index XORed with n % 8.  Call with NULL buffers to learn the sizes. */
+typedef struct {
+    uint8_t  hbits[8];
+    uint64_t num_tiles;
+    uint32_t block_begin;
+    uint32_t num_blocks;
+} mlb_fused_pass_t;
+typedef struct {
+    uint8_t  pos[5];
+    uint8_t  rows[8];
+    uint8_t  reserved[3];
+    uint32_t image;
+} mlb_fused_block_t;
+int  mlb_fused_plan(const mlb_op_t *ops, size_t num_ops, uint32_t num_qubits,
+                    mlb_fused_pass_t *passes, size_t *num_passes, mlb_fused_block_t *blocks,
+                    size_t *num_blocks, void *images, size_t *image_bytes);
 int  mlb_total_kernel_launches(uint64_t *out);
 
 /* ---- batched adjoint gradient (hardware-efficient ansatz) ---------------- */

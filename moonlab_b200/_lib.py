@@ -48,6 +48,16 @@ class MlbJobDesc(C.Structure):
                 ("reserved", C.c_int32), ("rng_seed", C.c_uint64)]
 
 
+class MlbFusedPass(C.Structure):
+    _fields_ = [("hbits", C.c_uint8 * 8), ("num_tiles", C.c_uint64), ("block_begin", C.c_uint32),
+                ("num_blocks", C.c_uint32)]
+
+
+class MlbFusedBlock(C.Structure):
+    _fields_ = [("pos", C.c_uint8 * 5), ("rows", C.c_uint8 * 8), ("reserved", C.c_uint8 * 3),
+                ("image", C.c_uint32)]
+
+
 class QuantumState(C.Structure):
     """quantum_state_t (reference src/quantum/state.h:102-131)."""
     _fields_ = [("num_qubits", C.c_size_t), ("state_dim", C.c_size_t), ("amplitudes", C.c_void_p),
@@ -117,6 +127,9 @@ _SIGS = {
     "mlb_plan_ops": (C.c_int, [C.POINTER(MlbOp), C.c_size_t, C.c_uint32, C.c_int, C.c_int,
                                C.POINTER(MlbFlushStats)]),
     "mlb_total_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),
+    "mlb_fused_plan": (C.c_int, [C.POINTER(MlbOp), C.c_size_t, C.c_uint32, C.POINTER(MlbFusedPass),
+                                 C.POINTER(C.c_size_t), C.POINTER(MlbFusedBlock), C.POINTER(C.c_size_t),
+                                 C.c_void_p, C.POINTER(C.c_size_t)]),
     "mlb_hea_create": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_size_t, C.POINTER(C.c_uint64),
                                  C.POINTER(C.c_uint64), C.POINTER(C.c_double), C.c_int, C.c_int,
                                  C.POINTER(C.c_void_p)]),

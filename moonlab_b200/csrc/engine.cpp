@@ -20,6 +20,7 @@
 #include <string>
 #include <vector>
 
+#include "fused.h"
 #include "mlb_internal.h"
 #include "planner.h"
 
@@ -104,6 +105,10 @@ struct mlb_state {
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   bool timed_pending = false;
   mlb_flush_stats_t stats{};
+  // fused path: device error word of the tensor-core kernel and its host copy
+  int* d_ferr = nullptr;
+  int* h_ferr = nullptr;
+  bool ferr_pending = false;
 };
 
 namespace {
@@ -379,6 +384,49 @@ int upload_plan(mlb_state* s, const void* host, size_t bytes) {
   return MLB_OK;
 }
 
+// Fused complex64 path: dense <= 5-qubit blocks on the tensor cores.
+int flush_fused(mlb_state* s, const std::vector<mlb_op_t>& ops) {
+  fused::Plan P;
+  int rc = fused::plan(ops, s->n, P);
+  if (rc) return fail(rc, "fused path: an op spans more than 5 qubits or the state has < 13 qubits");
+  if (!s->d_ferr) {
+    cudaError_t e = cudaMalloc((void**)&s->d_ferr, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_ferr, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e, "fused error word");
+  }
+  // one upload: blocks, then operand images (16 KiB each, 16-byte aligned)
+  const size_t bb = P.dev_blocks.size() * sizeof(FusedBlockDev);
+  const size_t ioff = (bb + 255) & ~(size_t)255;
+  std::vector<unsigned char> blob(ioff + P.images.size());
+  std::memcpy(blob.data(), P.dev_blocks.data(), bb);
+  std::memcpy(blob.data() + ioff, P.images.data(), P.images.size());
+  rc = upload_plan(s, blob.data(), blob.size());
+  if (rc) return rc;
+  const FusedBlockDev* d_blocks = reinterpret_cast<const FusedBlockDev*>(s->d_plan);
+  const uint8_t* d_images = reinterpret_cast<const uint8_t*>(s->d_plan) + ioff;
+  cudaMemsetAsync(s->d_ferr, 0, sizeof(int), s->stream);
+  mlb_flush_stats_t st{};
+  if (s->timing) cudaEventRecord(s->t0, s->stream);
+  for (const auto& dp : P.dev_passes) {
+    rc = launch_fused_pass(s->amp, (int)s->n, dp, d_blocks, d_images, s->d_ferr, s->num_sms, s->stream);
+    if (rc) return fail(rc, "fused pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    st.passes++;
+    st.kernel_launches++;
+    st.bytes_moved += 2 * 8 * (1ull << s->n);
+  }
+  if (s->timing) {
+    cudaEventRecord(s->t1, s->stream);
+    s->timed_pending = true;
+  }
+  cudaMemcpyAsync(s->h_ferr, s->d_ferr, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+  s->ferr_pending = true;
+  st.ops = ops.size();
+  st.dense_blocks = P.dev_blocks.size();
+  st.segments = P.dev_blocks.size();
+  s->stats = st;
+  return MLB_OK;
+}
+
 int flush_impl(mlb_state* s) {
   if (s->queue.empty()) return MLB_OK;
   DeviceGuard dg(s->device);
@@ -408,6 +456,7 @@ int flush_impl(mlb_state* s) {
   }
   std::vector<mlb_op_t> ops = s->fuse1q ? fuse_1q_runs(s->queue, s->n) : s->queue;
   s->queue.clear();
+  if (s->mode == MLB_EXEC_FUSED) return flush_fused(s, ops);
   Planner pl{s->n, s->dtype, geo(s->dtype)};
   pl.plan(ops);
   // one upload: ops then segments
@@ -452,6 +501,10 @@ int enqueue(mlb_state* s, const mlb_op_t& op) {
 int sync_stream(mlb_state* s) {
   cudaError_t e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
+  if (s->ferr_pending) {
+    s->ferr_pending = false;
+    if (*s->h_ferr) return fail(MLB_ERR_TIMEOUT, "fused pass: tensor-core completion wait ran out");
+  }
   return MLB_OK;
 }
 
@@ -539,6 +592,8 @@ void mlb_state_free(mlb_state_t* s) {
   if (s->amp) cudaFree(s->amp);
   if (s->d_scratch) cudaFree(s->d_scratch);
   if (s->d_plan) cudaFree(s->d_plan);
+  if (s->d_ferr) cudaFree(s->d_ferr);
+  if (s->h_ferr) cudaFreeHost(s->h_ferr);
   if (s->h_plan) cudaFreeHost(s->h_plan);
   if (s->plan_ev) cudaEventDestroy(s->plan_ev);
   if (s->t0) cudaEventDestroy(s->t0);
@@ -594,8 +649,10 @@ int mlb_state_stream(const mlb_state_t* s, void** out) {
 }
 int mlb_state_set_exec_mode(mlb_state_t* s, int mode) {
   if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
-  if (mode != MLB_EXEC_TILED && mode != MLB_EXEC_EAGER)
+  if (mode != MLB_EXEC_TILED && mode != MLB_EXEC_EAGER && mode != MLB_EXEC_FUSED)
     return fail(MLB_ERR_NOT_SUPPORTED, "exec mode %d not available", mode);
+  if (mode == MLB_EXEC_FUSED && (s->dtype != MLB_C64 || s->n < 13))
+    return fail(MLB_ERR_NOT_SUPPORTED, "the fused path needs a complex64 state of >= 13 qubits");
   int rc = flush_impl(s);
   if (rc) return rc;
   s->mode = mode;
@@ -1093,6 +1150,48 @@ int mlb_plan_ops(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fus
   st.kernel_launches = pl.passes.size();
   st.bytes_moved = st.passes * 2ull * (dtype == MLB_C128 ? 16ull : 8ull) * (1ull << n);
   *out = st;
+  return MLB_OK;
+}
+
+int mlb_fused_plan(const mlb_op_t* ops, size_t num, uint32_t n, mlb_fused_pass_t* passes,
+                   size_t* num_passes, mlb_fused_block_t* blocks, size_t* num_blocks, void* images,
+                   size_t* image_bytes) {
+  if ((!ops && num) || !num_passes || !num_blocks || !image_bytes)
+    return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (n < 13 || n > 34) return fail(MLB_ERR_NOT_SUPPORTED, "the fused path needs 13..34 qubits");
+  mlb_state probe;
+  probe.n = n;
+  std::vector<mlb_op_t> q;
+  q.reserve(num);
+  for (size_t i = 0; i < num; i++) {
+    int rc = validate(&probe, ops[i]);
+    if (rc) return rc;
+    q.push_back(canonical(ops[i]));
+  }
+  std::vector<mlb_op_t> f1 = fuse_1q_runs(q, n);
+  fused::Plan P;
+  int rc = fused::plan(f1, n, P);
+  if (rc) return fail(rc, "an op spans more than 5 qubits");
+  const bool fit = passes && blocks && images && *num_passes >= P.dev_passes.size() &&
+                   *num_blocks >= P.dev_blocks.size() && *image_bytes >= P.images.size();
+  *num_passes = P.dev_passes.size();
+  *num_blocks = P.dev_blocks.size();
+  *image_bytes = P.images.size();
+  if (!fit) return passes || blocks || images ? fail(MLB_ERR_INVALID_ARG, "buffers too small") : MLB_OK;
+  for (size_t i = 0; i < P.dev_passes.size(); i++) {
+    const auto& d = P.dev_passes[i];
+    std::memcpy(passes[i].hbits, d.hbits, 8);
+    passes[i].num_tiles = d.num_tiles;
+    passes[i].block_begin = d.block_begin;
+    passes[i].num_blocks = d.num_blocks;
+  }
+  for (size_t i = 0; i < P.dev_blocks.size(); i++) {
+    const auto& d = P.dev_blocks[i];
+    std::memcpy(blocks[i].pos, d.pos, 5);
+    std::memcpy(blocks[i].rows, d.q, 8);
+    blocks[i].image = d.image;
+  }
+  std::memcpy(images, P.images.data(), P.images.size());
   return MLB_OK;
 }
 

@@ -150,4 +150,27 @@ void count_launch(uint64_t k = 1);
 // Records the message mlb_last_error() returns on this thread; returns code.
 int record_error(int code, const char* msg);
 
+// ---- fused complex64 path (kernels_fused.cu, planned by fused.h) ----------
+// A dense 5-qubit block inside a 13-qubit tile: pos = its tile bit positions
+// (block index bit j <-> tile bit pos[j]), q = the other 8 tile positions in
+// increasing order (row index bit i <-> tile bit q[i]), image = index of its
+// 16 KiB operand image (bf16 hi then lo, K-major 128-byte swizzle).
+struct FusedBlockDev {
+  uint8_t pos[5];
+  uint8_t q[8];
+  uint8_t pad[3];
+  uint32_t image;
+};
+// A fused pass: tile = qubits 0..4 plus hbits[0..7]; blocks
+// [block_begin, block_begin + num_blocks) applied in order to every tile.
+struct FusedPassDev {
+  uint8_t hbits[8];
+  uint64_t num_tiles;
+  uint32_t block_begin;
+  uint32_t num_blocks;
+};
+// d_err: device word set non-zero if a tensor-core completion wait ran out.
+int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,
+                      const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream);
+
 }  // namespace mlb

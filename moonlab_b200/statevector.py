@@ -222,3 +222,26 @@ def gates_to_ops(gates: np.ndarray, n: int):
     check(lib.mlb_gates_to_ops(g.ctypes.data_as(C.POINTER(MlbGate)), len(g), n, ops, C.byref(cnt)),
           "mlb_gates_to_ops")
     return ops
+
+
+def fused_plan(gates: np.ndarray, n: int) -> dict:
+    """The fused complex64 path's plan for a circuit (host only): passes
+    (tile high qubits, block range), blocks (tile bit positions, row bits,
+    image index) and the bf16 operand images, as mlb_fused_plan returns them."""
+    from ._lib import MlbFusedBlock, MlbFusedPass
+    lib = load()
+    ops = gates_to_ops(gates, n)
+    np_, nb, ib = C.c_size_t(), C.c_size_t(), C.c_size_t()
+    check(lib.mlb_fused_plan(ops, len(ops), n, None, C.byref(np_), None, C.byref(nb), None, C.byref(ib)),
+          "mlb_fused_plan")
+    passes = (MlbFusedPass * np_.value)()
+    blocks = (MlbFusedBlock * nb.value)()
+    images = np.empty(ib.value, dtype=np.uint8)
+    check(lib.mlb_fused_plan(ops, len(ops), n, passes, C.byref(np_), blocks, C.byref(nb),
+                             images.ctypes.data_as(C.c_void_p), C.byref(ib)), "mlb_fused_plan")
+    return {
+        "passes": [{"hbits": list(p.hbits), "num_tiles": p.num_tiles, "block_begin": p.block_begin,
+                    "num_blocks": p.num_blocks} for p in passes],
+        "blocks": [{"pos": list(b.pos), "rows": list(b.rows), "image": b.image} for b in blocks],
+        "images": images,
+    }
