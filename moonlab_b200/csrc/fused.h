@@ -44,6 +44,7 @@ constexpr int kLowBits = 5;
 constexpr int kHighBits = kTileBits - kLowBits;
 constexpr int kBlockQubits = 5;
 constexpr size_t kBImageBytes = 16384;  // hi (8 KiB) + lo (8 KiB)
+constexpr size_t kMaxPassBlocks = 64;   // blocks per launch (the kernel's offset tables)
 
 using cd = std::complex<double>;
 
@@ -192,8 +193,11 @@ inline int make_blocks(const std::vector<mlb_op_t>& ops, uint32_t n, std::vector
   return MLB_OK;
 }
 
-// Group blocks into passes (5 low + <= 8 high qubits), pad each pass to 8
-// high qubits, and emit the device program and operand images.
+inline int emit(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P,
+                const std::vector<std::vector<int>>& pass_blocks, const std::vector<uint64_t>& pass_h);
+
+// Group whole blocks into passes (5 low + <= 8 high qubits) and emit the
+// device program and operand images.
 inline int plan_passes(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P) {
   if (n < (uint32_t)kTileBits) return MLB_ERR_NOT_SUPPORTED;
   const uint64_t all = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
@@ -218,10 +222,34 @@ inline int plan_passes(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P) {
       }
       if (blocked == all) break;
     }
-    // pad to exactly 8 high qubits
-    for (uint32_t g = kLowBits; g < n && plan::popc(pp.hmask) < kHighBits; g++) pp.hmask |= 1ull << g;
     P.passes.push_back(std::move(pp));
     while (first < P.blocks.size() && placed[first]) first++;
+  }
+  std::vector<std::vector<int>> pb;
+  std::vector<uint64_t> ph;
+  for (auto& pp : P.passes) {
+    pb.push_back(pp.blocks);
+    ph.push_back(pp.hmask);
+  }
+  return emit(ops, n, P, pb, ph);
+}
+
+// Device program and operand images for passes (block lists, high masks);
+// each pass is padded to exactly 8 high qubits.
+inline int emit(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P,
+                const std::vector<std::vector<int>>& pass_blocks, const std::vector<uint64_t>& pass_h) {
+  P.passes.clear();
+  for (size_t i = 0; i < pass_blocks.size(); i++) {
+    uint64_t h = pass_h[i];
+    for (uint32_t g = kLowBits; g < n && plan::popc(h) < kHighBits; g++) h |= 1ull << g;
+    // at most kMaxPassBlocks per launch: longer runs become consecutive passes on the same tile
+    for (size_t b0 = 0; b0 < pass_blocks[i].size(); b0 += kMaxPassBlocks) {
+      PassPlan pp;
+      pp.hmask = h;
+      const size_t b1 = std::min(pass_blocks[i].size(), b0 + kMaxPassBlocks);
+      pp.blocks.assign(pass_blocks[i].begin() + b0, pass_blocks[i].begin() + b1);
+      P.passes.push_back(std::move(pp));
+    }
   }
   // device program
   P.dev_blocks.clear();
@@ -299,10 +327,60 @@ inline int plan_passes(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P) {
   return MLB_OK;
 }
 
+// Pass-first planning: choose each pass's tile over the ops (every qubit of
+// an op, controls included, inside the tile; greedy look-ahead in op order),
+// then fuse the pass's ops into blocks on the tile's 13 qubits.  Ops are
+// finer than blocks, so passes pack more work than grouping whole blocks.
 inline int plan(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P) {
-  int rc = make_blocks(ops, n, P.blocks);
-  if (rc) return rc;
-  return plan_passes(ops, n, P);
+  if (n < (uint32_t)kTileBits) return MLB_ERR_NOT_SUPPORTED;
+  const uint64_t all = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
+  const uint64_t low = (1ull << kLowBits) - 1ull;
+  std::vector<uint64_t> qm(ops.size());
+  for (size_t i = 0; i < ops.size(); i++) {
+    qm[i] = plan::op_qubits(ops[i]);
+    if (plan::popc(qm[i]) > kBlockQubits) return MLB_ERR_NOT_SUPPORTED;
+  }
+  std::vector<char> placed(ops.size(), 0);
+  size_t first = 0;
+  P.blocks.clear();
+  std::vector<std::vector<int>> pass_blocks;
+  std::vector<uint64_t> pass_h;
+  while (first < ops.size()) {
+    uint64_t hmask = 0, blocked = 0;
+    std::vector<int> mine;
+    for (size_t i = first; i < ops.size(); i++) {
+      if (placed[i]) continue;
+      const uint64_t q = qm[i];
+      if (q & blocked) {
+        blocked |= q;
+      } else if (plan::popc(hmask | (q & ~low)) <= kHighBits) {
+        hmask |= q & ~low;
+        mine.push_back((int)i);
+        placed[i] = 1;
+      } else {
+        blocked |= q;
+      }
+      if (blocked == all) break;
+    }
+    while (first < ops.size() && placed[first]) first++;
+    // blocks over this pass's ops (their order is a valid order of the pass)
+    std::vector<mlb_op_t> sub;
+    sub.reserve(mine.size());
+    for (int i : mine) sub.push_back(ops[i]);
+    std::vector<Block> bl;
+    int rc = make_blocks(sub, n, bl);
+    if (rc) return rc;
+    std::vector<int> ids;
+    for (auto& b : bl) {
+      for (auto& oi : b.ops) oi = mine[oi];  // back to indices into ops
+      ids.push_back((int)P.blocks.size());
+      P.blocks.push_back(std::move(b));
+    }
+    pass_blocks.push_back(std::move(ids));
+    pass_h.push_back(hmask);
+  }
+  // reuse plan_passes' emission by presetting the pass list
+  return emit(ops, n, P, pass_blocks, pass_h);
 }
 
 }  // namespace fused

@@ -22,9 +22,14 @@
 // commit arrives every warp reads its 32 accumulator lanes back
 // (tcgen05.ld 32x32b, 64 columns) into the FP32 tile.
 //
-// The completion wait is bounded: if it runs out the kernel sets *err,
-// waits once more (bounded) for the MMAs in flight, frees its tensor memory
-// and returns.
+// Pipelining: the tile is double-buffered; while the tensor cores work on
+// tile t, 16-byte async copies (cp.async) bring tile t + grid into the other
+// buffer, so the HBM read overlaps the block math.  Each block's operand
+// image comes by one bulk copy completing on its own mbarrier, overlapping
+// the conversion of the amplitude operand.
+//
+// Waits are bounded: if one runs out the kernel sets *err, waits once more
+// (bounded) for what it issued, frees its tensor memory and returns.
 #include <atomic>
 
 #include <cuda_bf16.h>
@@ -41,13 +46,17 @@ constexpr int kTileAmps = 1 << 13;
 // shared-memory layout (bytes from a 1024-byte aligned base)
 constexpr uint32_t kAHi = 0;          // 256 rows x 128 B
 constexpr uint32_t kALo = 32768;
-constexpr uint32_t kBHi = 65536;      // 64 rows x 128 B
+constexpr uint32_t kBHi = 65536;      // 64 rows x 128 B, then lo
 constexpr uint32_t kBLo = 73728;
-constexpr uint32_t kTile = 81920;     // 2^13 float2 = 64 KiB
-constexpr uint32_t kMbar = 147456;
-constexpr uint32_t kTmemSlot = 147464;
-constexpr uint32_t kFlag = 147468;
-constexpr uint32_t kSmemUsed = 147472;
+constexpr uint32_t kTile0 = 81920;    // two tile buffers of 2^13 float2 (64 KiB each)
+constexpr uint32_t kTileBytes = 65536;
+constexpr uint32_t kMbarMma = 212992;
+constexpr uint32_t kMbarB = 213000;
+constexpr uint32_t kTmemSlot = 213008;
+constexpr uint32_t kFlag = 213012;
+constexpr uint32_t kRoff = 213024;    // per block: 32 swizzled column offsets (uint16), 16-byte aligned
+constexpr int kMaxBlocks = 64;        // blocks per pass (the planner splits longer passes)
+constexpr uint32_t kSmemUsed = kRoff + kMaxBlocks * 64;
 constexpr uint32_t kSmemBytes = kSmemUsed + 1024;  // alignment slack
 constexpr uint32_t kTmemCols = 128;
 constexpr long long kWaitLimit = 1ll << 22;      // try_wait rounds before giving up
@@ -101,6 +110,25 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
   return false;
 }
 
+// 16 KiB operand image (global, L2-resident) -> shared memory by one bulk
+// copy that completes on mbarrier `bar` (one thread).
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "{\n\t"
+      ".reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 st, [%0], %1;\n\t"
+      "}\n" ::"r"(bar),
+      "r"(bytes)
+      : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
   uint32_t* r = reinterpret_cast<uint32_t*>(v);
   asm volatile(
@@ -122,8 +150,10 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
-// XOR swizzle of the FP32 tile: spreads rows of any stride over the banks.
-__device__ __forceinline__ uint32_t tsw(uint32_t e) { return e ^ (((e >> 5) ^ (e >> 10)) & 31u); }
+// XOR swizzle of the FP32 tile on bits 1..4 (pairs of amplitudes stay
+// together, so 16-byte async copies land whole): spreads rows of any stride
+// over the banks.
+__device__ __forceinline__ uint32_t tsw(uint32_t e) { return e ^ ((((e >> 5) ^ (e >> 9)) & 15u) << 1); }
 
 __device__ __forceinline__ uint32_t deposit8(uint32_t v, const uint8_t (&pos)[8]) {
   uint32_t r = 0;
@@ -137,16 +167,34 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
+__device__ __forceinline__ uint64_t tile_base(uint64_t t, uint64_t tmask) {
+  uint64_t gbase = 0, v = t, m = tmask;
+  while (v && m) {
+    const uint64_t low = m & (~m + 1);
+    if (v & 1ull) gbase |= low;
+    v >>= 1;
+    m &= m - 1;
+  }
+  return gbase;
+}
+
+// Amplitude pair (e, e+1) of a tile -> its global index.
+__device__ __forceinline__ uint64_t tile_global(uint64_t gbase, uint32_t e, const FusedPassDev& pass) {
+  uint64_t g = gbase | (e & 31u);
+#pragma unroll
+  for (int h = 0; h < 8; h++) g |= (uint64_t)((e >> (5 + h)) & 1u) << pass.hbits[h];
+  return g;
+}
+
 __global__ void __launch_bounds__(kFThreads, 1)
     k_fused(float2* __restrict__ amp, FusedPassDev pass, const FusedBlockDev* __restrict__ blocks,
             const uint8_t* __restrict__ images, int* __restrict__ err) {
   extern __shared__ uint8_t smraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
   const uint32_t sbase = smem_u32(sm);
-  float2* tile = reinterpret_cast<float2*>(sm + kTile);
   volatile int* flag = reinterpret_cast<volatile int*>(sm + kFlag);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t bar = sbase + kMbar;
+  const uint32_t bar_mma = sbase + kMbarMma, bar_b = sbase + kMbarB;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + kTmemSlot),
@@ -154,7 +202,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_mma), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_b), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     *flag = 0;
   }
@@ -162,59 +211,66 @@ __global__ void __launch_bounds__(kFThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTmemSlot);
 
-  // high tile bits -> global qubits; the remaining qubits enumerate tiles
+  // Column offsets of every block of the pass, swizzled once: tsw is linear
+  // over GF(2), so tsw(row | col) = tsw(row) ^ tsw(col) for disjoint bits.
+  uint16_t* roff_tab = reinterpret_cast<uint16_t*>(sm + kRoff);
+  for (uint32_t i = tid; i < pass.num_blocks * 32u; i += kFThreads) {
+    const FusedBlockDev blk = blocks[pass.block_begin + i / 32u];
+    const uint32_t r = i & 31u;
+    uint32_t o = 0;
+#pragma unroll
+    for (int j = 0; j < 5; j++) o |= ((r >> j) & 1u) << blk.pos[j];
+    roff_tab[i] = (uint16_t)tsw(o);
+  }
+  __syncthreads();
+
   uint64_t hmask = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) hmask |= 1ull << pass.hbits[i];
   const uint64_t tmask = ~(hmask | 31ull);
 
-  uint32_t phase = 0;
-  bool bad = false;
-  for (uint64_t t = blockIdx.x; t < pass.num_tiles && !bad; t += gridDim.x) {
-    // global base of tile t: deposit t over the qubits outside the tile
-    uint64_t gbase = 0;
-    {
-      uint64_t v = t, m = tmask;
-      while (v && m) {
-        const uint64_t low = m & (~m + 1);
-        if (v & 1ull) gbase |= low;
-        v >>= 1;
-        m &= m - 1;
-      }
-    }
-    // load: pairs of amplitudes (16 B), 32 contiguous per high combination
+  // prefetch of a tile into buffer `buf`: 16 async 16-byte copies per thread
+  auto prefetch = [&](uint64_t t, int buf) {
+    const uint64_t gbase = tile_base(t, tmask);
+    const uint32_t dst0 = sbase + kTile0 + (uint32_t)buf * kTileBytes;
 #pragma unroll 4
     for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) {
       const uint32_t e = (uint32_t)(i * kFThreads + tid) * 2u;
-      uint64_t g = gbase | (e & 31u);
-#pragma unroll
-      for (int h = 0; h < 8; h++) g |= (uint64_t)((e >> (5 + h)) & 1u) << pass.hbits[h];
-      const float4 v = __ldcs(reinterpret_cast<const float4*>(amp + g));
-      tile[tsw(e)] = make_float2(v.x, v.y);
-      tile[tsw(e + 1)] = make_float2(v.z, v.w);
+      cp_async16(dst0 + tsw(e) * 8u, amp + tile_global(gbase, e, pass));
     }
-    __syncthreads();
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
 
-    for (uint32_t b = 0; b < pass.num_blocks && !bad; b++) {
+  uint32_t ph_mma = 0, ph_b = 0;
+  bool bad = false;
+  int buf = 0;
+  if ((uint64_t)blockIdx.x < pass.num_tiles) prefetch(blockIdx.x, 0);
+  for (uint64_t t = blockIdx.x; t < pass.num_tiles && !bad; t += gridDim.x, buf ^= 1) {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    if (t + gridDim.x < pass.num_tiles) prefetch(t + gridDim.x, buf ^ 1);
+    float2* tile = reinterpret_cast<float2*>(sm + kTile0 + (uint32_t)buf * kTileBytes);
+
+    for (uint32_t b = 0; b < pass.num_blocks; b++) {
       const FusedBlockDev blk = blocks[pass.block_begin + b];
-      // operand image of U' (hi, lo) -> shared memory, 16 KiB
-      {
-        const uint4* src = reinterpret_cast<const uint4*>(images + (size_t)blk.image * 16384);
-        uint4* dst = reinterpret_cast<uint4*>(sm + kBHi);
-#pragma unroll
-        for (int i = 0; i < 16384 / 16 / kFThreads; i++) dst[i * kFThreads + tid] = __ldg(src + i * kFThreads + tid);
-      }
+      if (tid == 0) bulk_load(sbase + kBHi, images + (size_t)blk.image * 16384, 16384, bar_b);
       // amplitude operand: this thread's row m = tid
       {
         const uint32_t m = (uint32_t)tid;
-        const uint32_t ebase = deposit8(m, blk.q);
+        const uint32_t ebase = tsw(deposit8(m, blk.q));
         uint32_t roff[32];
+        {
+          const uint4* rt = reinterpret_cast<const uint4*>(roff_tab + b * 32u);
 #pragma unroll
-        for (int r = 0; r < 32; r++) {
-          uint32_t o = 0;
+          for (int v = 0; v < 4; v++) {
+            const uint4 x = rt[v];
+            const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-          for (int j = 0; j < 5; j++) o |= (uint32_t)((r >> j) & 1) << blk.pos[j];
-          roff[r] = o;
+            for (int k = 0; k < 4; k++) {
+              roff[v * 8 + 2 * k] = w4[k] & 0xffffu;
+              roff[v * 8 + 2 * k + 1] = w4[k] >> 16;
+            }
+          }
         }
         uint8_t* ahi = sm + kAHi + m * 128;
         uint8_t* alo = sm + kALo + m * 128;
@@ -224,8 +280,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
           uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
           for (int w = 0; w < 4; w++) {
-            const float2 a0 = tile[tsw(ebase | roff[8 * c + 2 * w])];
-            const float2 a1 = tile[tsw(ebase | roff[8 * c + 2 * w + 1])];
+            const float2 a0 = tile[ebase ^ roff[8 * c + 2 * w]];
+            const float2 a1 = tile[ebase ^ roff[8 * c + 2 * w + 1]];
             const __nv_bfloat162 hre = __floats2bfloat162_rn(a0.x, a1.x);
             const __nv_bfloat162 him = __floats2bfloat162_rn(a0.y, a1.y);
             const float2 fre = __bfloat1622float2(hre), fim = __bfloat1622float2(him);
@@ -244,42 +300,55 @@ __global__ void __launch_bounds__(kFThreads, 1)
       __syncthreads();
 
       if (tid == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        bool ok = mbar_wait_bounded(bar_b, ph_b);  // operand image landed
+        if (ok) {
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
+          for (int h = 0; h < 2; h++) {
 #pragma unroll
-          for (int kc = 0; kc < 3; kc++) {
-            const uint32_t a0 = sbase + (kc == 1 ? kALo : kAHi) + (uint32_t)h * 16384u;
-            const uint32_t b0 = sbase + (kc == 2 ? kBLo : kBHi);
+            for (int kc = 0; kc < 3; kc++) {
+              const uint32_t a0 = sbase + (kc == 1 ? kALo : kAHi) + (uint32_t)h * 16384u;
+              const uint32_t b0 = sbase + (kc == 2 ? kBLo : kBHi);
 #pragma unroll
-            for (int kk = 0; kk < 4; kk++)
-              mma_bf16(tmem + (uint32_t)h * 64u, sdesc(a0 + kk * 32), sdesc(b0 + kk * 32),
-                       (kc | kk) != 0 ? 1u : 0u);
+              for (int kk = 0; kk < 4; kk++)
+                mma_bf16(tmem + (uint32_t)h * 64u, sdesc(a0 + kk * 32), sdesc(b0 + kk * 32),
+                         (kc | kk) != 0 ? 1u : 0u);
+            }
           }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                           bar_mma)
+                       : "memory");
+          ok = mbar_wait_bounded(bar_mma, ph_mma);
+          if (!ok) *flag = 2;  // MMAs issued, completion not seen
+        } else {
+          *flag = 1;  // operand copy not seen
         }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
-                     : "memory");
-        if (!mbar_wait_bounded(bar, phase)) *flag = 1;
       }
       __syncthreads();
       if (*flag) {
         bad = true;
         break;
       }
-      phase ^= 1u;
+      ph_b ^= 1u;
+      ph_mma ^= 1u;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       {
         const uint32_t h = (uint32_t)warp >> 2, qd = (uint32_t)warp & 3u;
         float d[64];
         tmem_ld64(tmem + ((qd * 32u) << 16) + h * 64u, d);
         const uint32_t m = h * 128u + qd * 32u + (uint32_t)lane;
-        const uint32_t ebase = deposit8(m, blk.q);
+        const uint32_t ebase = tsw(deposit8(m, blk.q));
+        const uint4* rt = reinterpret_cast<const uint4*>(roff_tab + b * 32u);
 #pragma unroll
-        for (int r = 0; r < 32; r++) {
-          uint32_t o = 0;
+        for (int v = 0; v < 4; v++) {
+          const uint4 x = rt[v];
+          const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-          for (int j = 0; j < 5; j++) o |= (uint32_t)((r >> j) & 1) << blk.pos[j];
-          tile[tsw(ebase | o)] = make_float2(d[r], d[32 + r]);
+          for (int k = 0; k < 4; k++) {
+            const int r = v * 8 + 2 * k;
+            tile[ebase ^ (w4[k] & 0xffffu)] = make_float2(d[r], d[32 + r]);
+            tile[ebase ^ (w4[k] >> 16)] = make_float2(d[r + 1], d[32 + r + 1]);
+          }
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -288,24 +357,23 @@ __global__ void __launch_bounds__(kFThreads, 1)
     if (bad) break;
 
     // store
+    {
+      const uint64_t gbase = tile_base(t, tmask);
 #pragma unroll 4
-    for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) {
-      const uint32_t e = (uint32_t)(i * kFThreads + tid) * 2u;
-      uint64_t g = gbase | (e & 31u);
-#pragma unroll
-      for (int h = 0; h < 8; h++) g |= (uint64_t)((e >> (5 + h)) & 1u) << pass.hbits[h];
-      const float2 a = tile[tsw(e)], c = tile[tsw(e + 1)];
-      __stcs(reinterpret_cast<float4*>(amp + g), make_float4(a.x, a.y, c.x, c.y));
+      for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) {
+        const uint32_t e = (uint32_t)(i * kFThreads + tid) * 2u;
+        const float4 v = *reinterpret_cast<const float4*>(tile + tsw(e));
+        __stcs(reinterpret_cast<float4*>(amp + tile_global(gbase, e, pass)), v);
+      }
     }
-    __syncthreads();
   }
 
-  if (bad) {
-    if (tid == 0) {
-      atomicExch(err, 1);
-      mbar_wait_bounded(bar, phase);  // let MMAs in flight finish before freeing
-    }
-    __syncthreads();
+  // leave no async copy or MMA in flight
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  if (bad && tid == 0) {
+    atomicExch(err, 1);
+    if (*flag == 1) mbar_wait_bounded(bar_b, ph_b);
+    else mbar_wait_bounded(bar_mma, ph_mma);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
@@ -317,7 +385,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
 
 int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,
                       const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream) {
-  if (n < 13 || pass.num_blocks == 0) return MLB_ERR_INVALID_ARG;
+  if (n < 13 || pass.num_blocks == 0 || pass.num_blocks > (uint32_t)kMaxBlocks) return MLB_ERR_INVALID_ARG;
   static std::atomic<uint64_t> attr_set_mask{0};
   int dev = 0;
   cudaGetDevice(&dev);
