@@ -287,34 +287,50 @@ def run_b200(args, ws, rank, local):
     h2d = gates.nbytes + shots.nbytes
     d2h = ez.nbytes + outs.nbytes
 
-    # complex64 on the same circuit, and its fidelity against complex128
-    s64 = StateVector(n, "c64", device=local)
-    s64.set_timing(True)
-    t64 = []
-    for i in range(args.warmup + max(1, min(args.steps, 3))):
-        s64.reset()
-        s64.run(gates)
-        s64.flush()
-        st64 = s64.flush_stats()
-        if i >= args.warmup:
-            t64.append(st64["gpu_ms"] / 1e3)
-    c64_s = statistics.median(t64)
+    # complex64 on the same circuit (plain tile passes, and the fused
+    # tensor-core path), each against the complex128 result
     sv.reset()
     sv.run(gates)
     sv.synchronize()
-    a = torch.as_tensor(_DeviceView(sv.device_ptr(), 1 << n, "<c16"), device=f"cuda:{local}")
-    b = torch.as_tensor(_DeviceView(s64.device_ptr(), 1 << n, "<c8"), device=f"cuda:{local}")
-    fid = 0.0
-    maxerr = 0.0
-    chunk = 1 << 26
-    ip = torch.zeros((), dtype=torch.complex128, device=f"cuda:{local}")
-    for off in range(0, 1 << n, chunk):
-        bb = b[off:off + chunk].to(torch.complex128)
-        aa = a[off:off + chunk]
-        ip += torch.vdot(aa, bb)
-        maxerr = max(maxerr, float((aa - bb).abs().max().item()))
-    fid = float(ip.abs().item() ** 2)
-    s64.close()
+    ref128 = torch.as_tensor(_DeviceView(sv.device_ptr(), 1 << n, "<c16"), device=f"cuda:{local}")
+
+    def c64_leg(mode):
+        s64 = StateVector(n, "c64", device=local)
+        s64.set_exec_mode(mode)
+        s64.set_timing(True)
+        t64, st64 = [], None
+        for i in range(args.warmup + max(1, min(args.steps, 3))):
+            s64.reset()
+            s64.run(gates)
+            s64.flush()
+            st64 = s64.flush_stats()
+            if i >= args.warmup:
+                t64.append(st64["gpu_ms"] / 1e3)
+        b = torch.as_tensor(_DeviceView(s64.device_ptr(), 1 << n, "<c8"), device=f"cuda:{local}")
+        ip = torch.zeros((), dtype=torch.complex128, device=f"cuda:{local}")
+        nb, maxerr = 0.0, 0.0
+        chunk = 1 << 26
+        for off in range(0, 1 << n, chunk):
+            bb = b[off:off + chunk].to(torch.complex128)
+            aa = ref128[off:off + chunk]
+            ip += torch.vdot(aa, bb)
+            nb += float(torch.vdot(bb, bb).real.item())
+            maxerr = max(maxerr, float((aa - bb).abs().max().item()))
+        s64.close()
+        secs = statistics.median(t64)
+        per_pass = secs / max(1, st64["passes"])
+        gbs = 2 * 8 * (1 << n) / per_pass / 1e9
+        return {"circuit_ms": secs * 1e3, "speedup_vs_c128": t_max / secs,
+                "fidelity": float(ip.abs().item() ** 2) / nb, "norm": nb, "max_amp_err": maxerr,
+                "passes": int(st64["passes"]), "dense_blocks": int(st64["dense_blocks"]),
+                "hbm_gbs_per_pass": gbs, "hbm_frac": gbs / peak}
+
+    c64 = c64_leg("tiled")
+    c64["path"] = "c64 tiled (CUDA cores)"
+    fused = c64_leg("fused")
+    fused["path"] = ("c64 fused: <=5-qubit dense blocks on tcgen05 tensor cores, split-bf16 products, "
+                     "FP32 accumulation; fidelity = |<psi128|psi64>|^2 / <psi64|psi64>")
+    fused["kernel"] = "k_fused"
 
     serving = None if args.no_serving else serving_leg(args, local)
 
@@ -341,8 +357,8 @@ def run_b200(args, ws, rank, local):
                          "frac": achieved / peak, "traffic": profiled_traffic(n),
                          "kernel": "k_tile<double>", "peak_source": peak_kind,
                          "algorithmic_bytes_per_pass": per_pass_bytes},
-            "c64": {"circuit_ms": c64_s * 1e3, "speedup_vs_c128": t_max / c64_s, "fidelity": fid,
-                    "max_amp_err": maxerr, "path": "c64 tiled"},
+            "c64": c64,
+            "fused_c64": fused,
             "e2e": {"value": ws / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
