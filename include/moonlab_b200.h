@@ -290,8 +290,8 @@ int  mlb_state_set_timing(mlb_state_t *s, int enable);
 int  mlb_plan_ops(const mlb_op_t *ops, size_t num_ops, uint32_t num_qubits, int dtype,
                   int fuse1q, mlb_flush_stats_t *out);
 /* The fused complex64 path's plan for these ops, as a flush in MLB_EXEC_FUSED
- * mode would launch it (host only).  Passes: tile = qubits 0..4 plus
- * hbits[0..7] (tile bit 5 + i <-> hbits[i]); blocks
+ * mode would launch it (host only).  Passes: tile = qubits 0..num_low-1 plus
+ * hbits[0..num_high-1] (tile bit num_low + i <-> hbits[i]); blocks
  * [block_begin, block_begin + num_blocks) act on every tile in order.  A
  * block acts on tile bits pos[0..4] (block index bit j <-> pos[j]); rows
  * lists the other 8 tile bits.  Its operand image (16 KiB at image * 16384)
@@ -300,7 +300,10 @@ int  mlb_plan_ops(const mlb_op_t *ops, size_t num_ops, uint32_t num_qubits, int 
  * (n, k) at byte (n / 8) * 1024 + (n % 8) * 128 + 2 k with the 16-byte
  * chunk index XORed with n % 8.  Call with NULL buffers to learn the sizes. */
 typedef struct {
-    uint8_t  hbits[8];
+    uint8_t  hbits[12];
+    uint8_t  num_low;
+    uint8_t  num_high;
+    uint8_t  reserved[2];
     uint64_t num_tiles;
     uint32_t block_begin;
     uint32_t num_blocks;

@@ -49,7 +49,8 @@ class MlbJobDesc(C.Structure):
 
 
 class MlbFusedPass(C.Structure):
-    _fields_ = [("hbits", C.c_uint8 * 8), ("num_tiles", C.c_uint64), ("block_begin", C.c_uint32),
+    _fields_ = [("hbits", C.c_uint8 * 12), ("num_low", C.c_uint8), ("num_high", C.c_uint8),
+                ("reserved", C.c_uint8 * 2), ("num_tiles", C.c_uint64), ("block_begin", C.c_uint32),
                 ("num_blocks", C.c_uint32)]
 
 

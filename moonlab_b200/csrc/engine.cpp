@@ -1180,7 +1180,9 @@ int mlb_fused_plan(const mlb_op_t* ops, size_t num, uint32_t n, mlb_fused_pass_t
   if (!fit) return passes || blocks || images ? fail(MLB_ERR_INVALID_ARG, "buffers too small") : MLB_OK;
   for (size_t i = 0; i < P.dev_passes.size(); i++) {
     const auto& d = P.dev_passes[i];
-    std::memcpy(passes[i].hbits, d.hbits, 8);
+    std::memcpy(passes[i].hbits, d.hbits, 12);
+    passes[i].num_low = d.num_low;
+    passes[i].num_high = d.num_high;
     passes[i].num_tiles = d.num_tiles;
     passes[i].block_begin = d.block_begin;
     passes[i].num_blocks = d.num_blocks;

@@ -11,9 +11,8 @@
 // here runs of 1- and 2-qubit gates on up to 5 qubits collapse into one
 // 2^5 x 2^5 complex matrix.
 //
-// A tile pass holds the 5 low qubits and 8 chosen high qubits (2^13
-// amplitudes, 64 KiB of complex64); it takes blocks in order, with the same
-// look-ahead, while their qubits fit.  Blocks on fewer than 5 qubits are
+// A tile pass holds the 4 low qubits (128-byte contiguous runs) and 9 chosen
+// high qubits (2^13 amplitudes, 64 KiB of complex64).  Blocks on fewer than 5 qubits are
 // padded with other tile qubits (identity on them).
 //
 // Operand: for a block U (32x32 complex), the real 64x64 matrix
@@ -40,7 +39,7 @@ namespace mlb {
 namespace fused {
 
 constexpr int kTileBits = 13;     // 2^13 complex64 amplitudes per tile
-constexpr int kLowBits = 5;
+constexpr int kLowBits = 4;       // 16 contiguous amplitudes (128 B) per tile row
 constexpr int kHighBits = kTileBits - kLowBits;
 constexpr int kBlockQubits = 5;
 constexpr size_t kBImageBytes = 16384;  // hi (8 KiB) + lo (8 KiB)
@@ -54,7 +53,7 @@ struct Block {
 };
 
 struct PassPlan {
-  uint64_t hmask = 0;           // the 8 high tile qubits
+  uint64_t hmask = 0;           // the high tile qubits
   std::vector<int> blocks;      // indices into the block list
 };
 
@@ -257,6 +256,8 @@ inline int emit(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P,
   P.images.clear();
   for (const auto& pp : P.passes) {
     FusedPassDev dp{};
+    dp.num_low = (uint8_t)kLowBits;
+    dp.num_high = (uint8_t)kHighBits;
     int tile_pos[64];
     for (int g = 0; g < 64; g++) tile_pos[g] = -1;
     for (int g = 0; g < kLowBits; g++) tile_pos[g] = g;
@@ -345,23 +346,52 @@ inline int plan(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P) {
   P.blocks.clear();
   std::vector<std::vector<int>> pass_blocks;
   std::vector<uint64_t> pass_h;
-  while (first < ops.size()) {
-    uint64_t hmask = 0, blocked = 0;
-    std::vector<int> mine;
+  // One pass from the unplaced ops, in order: an op joins if all its qubits
+  // fit the tile (growing the high set up to 8 when `grow`) and no skipped
+  // op shares a qubit with it.
+  auto run = [&](uint64_t hmask, bool grow, std::vector<int>* taken) {
+    uint64_t blocked = 0;
+    int cnt = 0;
     for (size_t i = first; i < ops.size(); i++) {
       if (placed[i]) continue;
       const uint64_t q = qm[i];
+      const uint64_t need = q & ~low & ~hmask;
       if (q & blocked) {
         blocked |= q;
-      } else if (plan::popc(hmask | (q & ~low)) <= kHighBits) {
-        hmask |= q & ~low;
-        mine.push_back((int)i);
-        placed[i] = 1;
+      } else if (need == 0 || (grow && plan::popc(hmask | need) <= kHighBits)) {
+        hmask |= need;
+        cnt++;
+        if (taken) taken->push_back((int)i);
       } else {
         blocked |= q;
       }
       if (blocked == all) break;
     }
+    return std::make_pair(cnt, hmask);
+  };
+  while (first < ops.size()) {
+    // strategy A: first come; strategy B: the 8 high qubits most used by
+    // the next ops (weighted toward the front); keep the one placing more
+    const auto A = run(0, true, nullptr);
+    std::vector<double> score(n, 0.0);
+    int seen = 0;
+    for (size_t i = first; i < ops.size() && seen < 8 * (int)n; i++) {
+      if (placed[i]) continue;
+      const uint64_t q = qm[i] & ~low;
+      for (uint32_t b = 0; b < n; b++)
+        if (q >> b & 1ull) score[b] += 1.0 / (1.0 + seen * 0.02);
+      seen++;
+    }
+    std::vector<int> order;
+    for (uint32_t b = kLowBits; b < n; b++) order.push_back((int)b);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return score[a] > score[b]; });
+    uint64_t hb = 0;
+    for (int k = 0; k < (int)order.size() && k < kHighBits; k++)
+      if (score[order[k]] > 0) hb |= 1ull << order[k];
+    const auto Bs = run(hb, true, nullptr);
+    std::vector<int> mine;
+    const uint64_t hmask = (Bs.first > A.first ? run(hb, true, &mine) : run(0, true, &mine)).second;
+    for (int i : mine) placed[i] = 1;
     while (first < ops.size() && placed[first]) first++;
     // blocks over this pass's ops (their order is a valid order of the pass)
     std::vector<mlb_op_t> sub;

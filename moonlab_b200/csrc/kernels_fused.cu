@@ -3,7 +3,7 @@
 // FP32 accumulation in tensor memory.
 //
 // One pass streams the state once through shared memory in tiles of 2^13
-// amplitudes (qubits 0..4 plus 8 chosen high qubits).  For a block acting on
+// amplitudes (the low qubits, contiguous in memory, plus chosen high qubits).  For a block acting on
 // tile bits P (5 of them) the tile is a 256 x 32 complex matrix T[m][r]
 // (m over the other 8 tile bits, r over P) and the block computes
 // T <- T U^T.  In real arithmetic with A = [Re T | Im T] (256 x 64) and
@@ -56,7 +56,8 @@ constexpr uint32_t kTmemSlot = 213008;
 constexpr uint32_t kFlag = 213012;
 constexpr uint32_t kRoff = 213024;    // per block: 32 swizzled column offsets (uint16), 16-byte aligned
 constexpr int kMaxBlocks = 64;        // blocks per pass (the planner splits longer passes)
-constexpr uint32_t kSmemUsed = kRoff + kMaxBlocks * 64;
+constexpr uint32_t kHiDep = kRoff + kMaxBlocks * 64;  // 16 x uint64: global offsets of tile bits 9..12
+constexpr uint32_t kSmemUsed = kHiDep + 16 * 8;
 constexpr uint32_t kSmemBytes = kSmemUsed + 1024;  // alignment slack
 constexpr uint32_t kTmemCols = 128;
 constexpr long long kWaitLimit = 1ll << 22;      // try_wait rounds before giving up
@@ -180,9 +181,11 @@ __device__ __forceinline__ uint64_t tile_base(uint64_t t, uint64_t tmask) {
 
 // Amplitude pair (e, e+1) of a tile -> its global index.
 __device__ __forceinline__ uint64_t tile_global(uint64_t gbase, uint32_t e, const FusedPassDev& pass) {
-  uint64_t g = gbase | (e & 31u);
+  const uint32_t L = pass.num_low;
+  uint64_t g = gbase | (e & ((1u << L) - 1u));
 #pragma unroll
-  for (int h = 0; h < 8; h++) g |= (uint64_t)((e >> (5 + h)) & 1u) << pass.hbits[h];
+  for (int h = 0; h < 12; h++)
+    if (h < (int)pass.num_high) g |= (uint64_t)((e >> (L + h)) & 1u) << pass.hbits[h];
   return g;
 }
 
@@ -222,22 +225,31 @@ __global__ void __launch_bounds__(kFThreads, 1)
     for (int j = 0; j < 5; j++) o |= ((r >> j) & 1u) << blk.pos[j];
     roff_tab[i] = (uint16_t)tsw(o);
   }
+  if (tid < kTileAmps / 2 / kFThreads)
+    reinterpret_cast<uint64_t*>(sm + kHiDep)[tid] = tile_global(0, (uint32_t)tid * 2u * kFThreads, pass);
   __syncthreads();
 
-  uint64_t hmask = 0;
+  uint64_t hmask = (1ull << pass.num_low) - 1ull;
 #pragma unroll
-  for (int i = 0; i < 8; i++) hmask |= 1ull << pass.hbits[i];
-  const uint64_t tmask = ~(hmask | 31ull);
+  for (int i = 0; i < 12; i++)
+    if (i < (int)pass.num_high) hmask |= 1ull << pass.hbits[i];
+  const uint64_t tmask = ~hmask;
+
+  // Tile-local index e of this thread's i-th amplitude pair: e = 512 i + 2 tid.
+  // Its global offset is linear in e over disjoint bits, so it splits into
+  // a per-thread part (bits 0..8) and a per-i part (bits 9..12, shared table).
+  const uint64_t my_off = tile_global(0, 2u * (uint32_t)tid, pass);
+  const uint64_t* hidep = reinterpret_cast<const uint64_t*>(sm + kHiDep);
+  uint32_t my_sw[kTileAmps / 2 / kFThreads];
+#pragma unroll
+  for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) my_sw[i] = tsw((uint32_t)(i * kFThreads + tid) * 2u);
 
   // prefetch of a tile into buffer `buf`: 16 async 16-byte copies per thread
   auto prefetch = [&](uint64_t t, int buf) {
-    const uint64_t gbase = tile_base(t, tmask);
+    const uint64_t gb = tile_base(t, tmask) | my_off;
     const uint32_t dst0 = sbase + kTile0 + (uint32_t)buf * kTileBytes;
-#pragma unroll 4
-    for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) {
-      const uint32_t e = (uint32_t)(i * kFThreads + tid) * 2u;
-      cp_async16(dst0 + tsw(e) * 8u, amp + tile_global(gbase, e, pass));
-    }
+#pragma unroll
+    for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) cp_async16(dst0 + my_sw[i] * 8u, amp + (gb | hidep[i]));
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
 
@@ -245,6 +257,10 @@ __global__ void __launch_bounds__(kFThreads, 1)
   bool bad = false;
   int buf = 0;
   if ((uint64_t)blockIdx.x < pass.num_tiles) prefetch(blockIdx.x, 0);
+  // operand image of the first block; each later one is requested as soon as
+  // the MMAs reading the previous one have completed
+  if (tid == 0 && (uint64_t)blockIdx.x < pass.num_tiles)
+    bulk_load(sbase + kBHi, images + (size_t)blocks[pass.block_begin].image * 16384, 16384, bar_b);
   for (uint64_t t = blockIdx.x; t < pass.num_tiles && !bad; t += gridDim.x, buf ^= 1) {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
@@ -253,7 +269,6 @@ __global__ void __launch_bounds__(kFThreads, 1)
 
     for (uint32_t b = 0; b < pass.num_blocks; b++) {
       const FusedBlockDev blk = blocks[pass.block_begin + b];
-      if (tid == 0) bulk_load(sbase + kBHi, images + (size_t)blk.image * 16384, 16384, bar_b);
       // amplitude operand: this thread's row m = tid
       {
         const uint32_t m = (uint32_t)tid;
@@ -319,7 +334,15 @@ __global__ void __launch_bounds__(kFThreads, 1)
                            bar_mma)
                        : "memory");
           ok = mbar_wait_bounded(bar_mma, ph_mma);
-          if (!ok) *flag = 2;  // MMAs issued, completion not seen
+          if (!ok) {
+            *flag = 2;  // MMAs issued, completion not seen
+          } else {
+            // next operand image: next block of this tile, or block 0 of the next tile
+            const bool more = b + 1 < pass.num_blocks || t + gridDim.x < pass.num_tiles;
+            const uint32_t nb = b + 1 < pass.num_blocks ? b + 1 : 0;
+            if (more)
+              bulk_load(sbase + kBHi, images + (size_t)blocks[pass.block_begin + nb].image * 16384, 16384, bar_b);
+          }
         } else {
           *flag = 1;  // operand copy not seen
         }
@@ -358,12 +381,11 @@ __global__ void __launch_bounds__(kFThreads, 1)
 
     // store
     {
-      const uint64_t gbase = tile_base(t, tmask);
-#pragma unroll 4
+      const uint64_t gb = tile_base(t, tmask) | my_off;
+#pragma unroll
       for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) {
-        const uint32_t e = (uint32_t)(i * kFThreads + tid) * 2u;
-        const float4 v = *reinterpret_cast<const float4*>(tile + tsw(e));
-        __stcs(reinterpret_cast<float4*>(amp + tile_global(gbase, e, pass)), v);
+        const float4 v = *reinterpret_cast<const float4*>(tile + my_sw[i]);
+        __stcs(reinterpret_cast<float4*>(amp + (gb | hidep[i])), v);
       }
     }
   }
@@ -385,7 +407,9 @@ __global__ void __launch_bounds__(kFThreads, 1)
 
 int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,
                       const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream) {
-  if (n < 13 || pass.num_blocks == 0 || pass.num_blocks > (uint32_t)kMaxBlocks) return MLB_ERR_INVALID_ARG;
+  if (n < 13 || pass.num_blocks == 0 || pass.num_blocks > (uint32_t)kMaxBlocks ||
+      pass.num_low < 1 || pass.num_low + pass.num_high != 13)
+    return MLB_ERR_INVALID_ARG;
   static std::atomic<uint64_t> attr_set_mask{0};
   int dev = 0;
   cudaGetDevice(&dev);

@@ -161,10 +161,15 @@ struct FusedBlockDev {
   uint8_t pad[3];
   uint32_t image;
 };
-// A fused pass: tile = qubits 0..4 plus hbits[0..7]; blocks
-// [block_begin, block_begin + num_blocks) applied in order to every tile.
+// A fused pass: tile = qubits 0..num_low-1 (tile bits 0..num_low-1) plus
+// hbits[0..num_high-1] (tile bits num_low + i), num_low + num_high = 13;
+// blocks [block_begin, block_begin + num_blocks) applied in order to every
+// tile.
 struct FusedPassDev {
-  uint8_t hbits[8];
+  uint8_t hbits[12];
+  uint8_t num_low;
+  uint8_t num_high;
+  uint8_t pad[2];
   uint64_t num_tiles;
   uint32_t block_begin;
   uint32_t num_blocks;

@@ -240,8 +240,8 @@ def fused_plan(gates: np.ndarray, n: int) -> dict:
     check(lib.mlb_fused_plan(ops, len(ops), n, passes, C.byref(np_), blocks, C.byref(nb),
                              images.ctypes.data_as(C.c_void_p), C.byref(ib)), "mlb_fused_plan")
     return {
-        "passes": [{"hbits": list(p.hbits), "num_tiles": p.num_tiles, "block_begin": p.block_begin,
-                    "num_blocks": p.num_blocks} for p in passes],
+        "passes": [{"hbits": list(p.hbits)[:p.num_high], "num_low": p.num_low, "num_tiles": p.num_tiles,
+                    "block_begin": p.block_begin, "num_blocks": p.num_blocks} for p in passes],
         "blocks": [{"pos": list(b.pos), "rows": list(b.rows), "image": b.image} for b in blocks],
         "images": images,
     }

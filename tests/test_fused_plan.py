@@ -45,13 +45,12 @@ def deposit(v, bits):
 def replay(plan, n, state):
     st = state.astype(np.complex128).copy()
     imgs = plan["images"].reshape(-1, 16384)
-    others = lambda hb: [q for q in range(n) if q >= 5 and q not in hb]
     e = np.arange(1 << 13, dtype=np.int64)
     for p in plan["passes"]:
-        hb = p["hbits"]
-        rest = others(hb)
+        hb, L = p["hbits"], p["num_low"]
+        rest = [q for q in range(n) if q >= L and q not in hb]
         t = np.arange(p["num_tiles"], dtype=np.int64)
-        G = deposit(t, rest)[:, None] | deposit(e, list(range(5)) + hb)[None, :]
+        G = deposit(t, rest)[:, None] | deposit(e, list(range(L)) + hb)[None, :]
         T = st[G]
         for blk in plan["blocks"][p["block_begin"]:p["block_begin"] + p["num_blocks"]]:
             idx = deposit(np.arange(256, dtype=np.int64), blk["rows"])[:, None] | \
@@ -80,7 +79,8 @@ def test_fused_plan_replays_the_circuit(n, depth):
     for b in plan["blocks"]:
         assert sorted(b["pos"] + b["rows"]) == list(range(13))
     for p in plan["passes"]:
-        assert len(set(p["hbits"])) == 8 and min(p["hbits"]) >= 5 and max(p["hbits"]) < n
+        L = p["num_low"]
+        assert len(set(p["hbits"])) == 13 - L and min(p["hbits"]) >= L and max(p["hbits"]) < n
     init = np.zeros(1 << n, dtype=np.complex128)
     init[0] = 1
     got = replay(plan, n, init)
