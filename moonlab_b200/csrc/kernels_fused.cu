@@ -50,10 +50,10 @@ constexpr uint32_t kBHi = 65536;      // 64 rows x 128 B, then lo
 constexpr uint32_t kBLo = 73728;
 constexpr uint32_t kTile0 = 81920;    // two tile buffers of 2^13 float2 (64 KiB each)
 constexpr uint32_t kTileBytes = 65536;
-constexpr uint32_t kMbarMma = 212992;
-constexpr uint32_t kMbarB = 213000;
-constexpr uint32_t kTmemSlot = 213008;
-constexpr uint32_t kFlag = 213012;
+constexpr uint32_t kMbarMma = 212992;  // two: one per 128-row half
+constexpr uint32_t kMbarB = 213008;
+constexpr uint32_t kTmemSlot = 213016;
+constexpr uint32_t kFlag = 213020;
 constexpr uint32_t kRoff = 213024;    // per block: 32 swizzled column offsets (uint16), 16-byte aligned
 constexpr int kMaxBlocks = 64;        // blocks per pass (the planner splits longer passes)
 constexpr uint32_t kHiDep = kRoff + kMaxBlocks * 64;  // 16 x uint64: global offsets of tile bits 9..12
@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
   const uint32_t sbase = smem_u32(sm);
   volatile int* flag = reinterpret_cast<volatile int*>(sm + kFlag);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t bar_mma = sbase + kMbarMma, bar_b = sbase + kMbarB;
+  const uint32_t bar_mma = sbase + kMbarMma, bar_b = sbase + kMbarB;  // bar_mma + 8 h: half h
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + kTmemSlot),
@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
   }
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_mma), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_mma + 8), "r"(1));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_b), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     *flag = 0;
@@ -315,8 +316,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
       __syncthreads();
 
       if (tid == 0) {
-        bool ok = mbar_wait_bounded(bar_b, ph_b);  // operand image landed
-        if (ok) {
+        if (mbar_wait_bounded(bar_b, ph_b)) {  // operand image landed
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
           for (int h = 0; h < 2; h++) {
@@ -329,24 +329,55 @@ __global__ void __launch_bounds__(kFThreads, 1)
                 mma_bf16(tmem + (uint32_t)h * 64u, sdesc(a0 + kk * 32), sdesc(b0 + kk * 32),
                          (kc | kk) != 0 ? 1u : 0u);
             }
+            // half h done -> its mbarrier (commit covers all earlier MMAs of this thread)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             bar_mma + 8u * (uint32_t)h)
+                         : "memory");
           }
-          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                           bar_mma)
-                       : "memory");
-          ok = mbar_wait_bounded(bar_mma, ph_mma);
-          if (!ok) {
-            *flag = 2;  // MMAs issued, completion not seen
-          } else {
-            // next operand image: next block of this tile, or block 0 of the next tile
+        } else {
+          atomicOr((int*)flag, 1);  // operand copy not seen; no MMA issued
+        }
+      }
+      // Each warp waits for the MMAs of its own half and reads its 32
+      // accumulator lanes back; half 0 overlaps the MMAs of half 1.  The
+      // lane that sees half 1 complete (all MMAs done, B free) requests the
+      // next operand image.
+      {
+        const uint32_t h = (uint32_t)warp >> 2, qd = (uint32_t)warp & 3u;
+        __syncwarp();
+        int ok = 0;
+        if (lane == 0 && !*flag) {
+          ok = mbar_wait_bounded(bar_mma + 8u * h, ph_mma) ? 1 : 0;
+          if (!ok) atomicOr((int*)flag, 2);
+          if (ok && h == 1 && qd == 0) {
             const bool more = b + 1 < pass.num_blocks || t + gridDim.x < pass.num_tiles;
             const uint32_t nb = b + 1 < pass.num_blocks ? b + 1 : 0;
             if (more)
               bulk_load(sbase + kBHi, images + (size_t)blocks[pass.block_begin + nb].image * 16384, 16384, bar_b);
           }
-        } else {
-          *flag = 1;  // operand copy not seen
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) {
+          asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          float d[64];
+          tmem_ld64(tmem + ((qd * 32u) << 16) + h * 64u, d);
+          const uint32_t m = h * 128u + qd * 32u + (uint32_t)lane;
+          const uint32_t ebase = tsw(deposit8(m, blk.q));
+          const uint4* rt = reinterpret_cast<const uint4*>(roff_tab + b * 32u);
+#pragma unroll
+          for (int v = 0; v < 4; v++) {
+            const uint4 x = rt[v];
+            const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const int r = v * 8 + 2 * k;
+              tile[ebase ^ (w4[k] & 0xffffu)] = make_float2(d[r], d[32 + r]);
+              tile[ebase ^ (w4[k] >> 16)] = make_float2(d[r + 1], d[32 + r + 1]);
+            }
+          }
         }
       }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       __syncthreads();
       if (*flag) {
         bad = true;
@@ -354,28 +385,6 @@ __global__ void __launch_bounds__(kFThreads, 1)
       }
       ph_b ^= 1u;
       ph_mma ^= 1u;
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      {
-        const uint32_t h = (uint32_t)warp >> 2, qd = (uint32_t)warp & 3u;
-        float d[64];
-        tmem_ld64(tmem + ((qd * 32u) << 16) + h * 64u, d);
-        const uint32_t m = h * 128u + qd * 32u + (uint32_t)lane;
-        const uint32_t ebase = tsw(deposit8(m, blk.q));
-        const uint4* rt = reinterpret_cast<const uint4*>(roff_tab + b * 32u);
-#pragma unroll
-        for (int v = 0; v < 4; v++) {
-          const uint4 x = rt[v];
-          const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-          for (int k = 0; k < 4; k++) {
-            const int r = v * 8 + 2 * k;
-            tile[ebase ^ (w4[k] & 0xffffu)] = make_float2(d[r], d[32 + r]);
-            tile[ebase ^ (w4[k] >> 16)] = make_float2(d[r + 1], d[32 + r + 1]);
-          }
-        }
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      __syncthreads();
     }
     if (bad) break;
 
@@ -392,10 +401,14 @@ __global__ void __launch_bounds__(kFThreads, 1)
 
   // leave no async copy or MMA in flight
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  if (bad && tid == 0) {
+  if (bad && tid == 0) {  // flag bit 1: operand copy pending; bit 2: MMAs pending
     atomicExch(err, 1);
-    if (*flag == 1) mbar_wait_bounded(bar_b, ph_b);
-    else mbar_wait_bounded(bar_mma, ph_mma);
+    const int f = *flag;
+    if (f & 1) mbar_wait_bounded(bar_b, ph_b);
+    if (f & 2) {
+      mbar_wait_bounded(bar_mma, ph_mma);
+      mbar_wait_bounded(bar_mma + 8, ph_mma);
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
