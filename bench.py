@@ -332,7 +332,10 @@ def run_b200(args, ws, rank, local):
                      "FP32 accumulation; fidelity = |<psi128|psi64>|^2 / <psi64|psi64>")
     fused["kernel"] = "k_fused"
 
+    sv.close()
     serving = None if args.no_serving else serving_leg(args, local)
+    sweep = None if args.no_sweep else gate_sweep_leg(local, peak)
+    vqe = None if args.no_vqe else vqe_leg(local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -367,8 +370,11 @@ def run_b200(args, ws, rank, local):
         }
         if serving is not None:
             line["serving"] = serving
+        if sweep is not None:
+            line["gate_sweep"] = sweep
+        if vqe is not None:
+            line["vqe_gradient"] = vqe
         print(json.dumps(line), flush=True)
-    sv.close()
 
 
 def serving_leg(args, local):
@@ -398,6 +404,76 @@ def serving_leg(args, local):
     }
 
 
+def gate_sweep_leg(local, peak):
+    """Per-gate HBM throughput on the per-gate kernels (one full sweep over
+    the amplitudes a gate touches), depth-20-circuit sizes 26..33 qubits in
+    complex128 and 26..34 in complex64: RX on low (0, 1, 2), middle (n/2) and
+    high (n-3 .. n-1) targets, CNOT and CRZ with the control below / above
+    the target.  GB/s = 2 x (bytes of the touched amplitudes) / device time
+    of the gate's kernel (CUDA events on the engine's stream), median of 3."""
+    from moonlab_b200 import StateVector
+    c, sn = math.cos(0.15), math.sin(0.15)
+    rx = np.array([[c, -1j * sn], [-1j * sn, c]])
+    xm = np.array([[0, 1], [1, 0]], dtype=np.complex128)
+    rz = np.diag([np.exp(-0.15j), np.exp(0.15j)])
+    out = {}
+    for dtype, ns in (("c128", (26, 28, 30, 32, 33)), ("c64", (26, 28, 30, 32, 34))):
+        out[dtype] = {}
+        for n in ns:
+            sv = StateVector(n, dtype, device=local)
+            sv.set_exec_mode("eager")
+            sv.set_timing(True)
+            mid = n // 2
+            cases = [("rx_low", [(lambda q=q: sv.apply_1q(q, rx)) for q in (0, 1, 2)]),
+                     ("rx_mid", [lambda: sv.apply_1q(mid, rx)]),
+                     ("rx_high", [(lambda q=q: sv.apply_1q(q, rx)) for q in (n - 3, n - 2, n - 1)]),
+                     ("cnot_ctrl_below", [lambda: sv.apply_controlled_1q([1], mid, xm)]),
+                     ("cnot_ctrl_above", [lambda: sv.apply_controlled_1q([n - 2], mid, xm)]),
+                     ("crz_ctrl_below", [lambda: sv.apply_controlled_1q([1], mid, rz)]),
+                     ("crz_ctrl_above", [lambda: sv.apply_controlled_1q([n - 2], mid, rz)])]
+            row = {}
+            for name, fns in cases:
+                rates = []
+                for f in fns:
+                    ts = []
+                    for rep in range(4):
+                        f()
+                        sv.flush()
+                        st = sv.flush_stats()
+                        if rep:
+                            ts.append(st["bytes_moved"] / (st["gpu_ms"] / 1e3) / 1e9)
+                    rates.append(statistics.median(ts))
+                row[name] = round(statistics.median(rates), 1)
+            row["frac_of_peak_rx_mid"] = round(row["rx_mid"] / peak, 3)
+            out[dtype][str(n)] = row
+            sv.close()
+    return out
+
+
+def vqe_leg(local):
+    """VQE adjoint gradient: hardware-efficient ansatz N = 20, L = 8 (320
+    parameters), 80 random 2-local Pauli terms, a batch of 256 parameter
+    vectors in one call, complex128 and complex64; host parameters in,
+    host energies and gradients out (timed end to end)."""
+    from moonlab_b200.circuits import config_c4
+    from moonlab_b200.vqe import HEAProblem
+    prob = config_c4(n=20, layers=8, batch=256, seed=0xC4)
+    res = {"workload": "HEA N=20 L=8 (320 parameters), 80 2-local Pauli terms, batch 256"}
+    grads = {}
+    for dt in ("c128", "c64"):
+        p = HEAProblem(20, 8, prob.coeffs, xmasks=prob.xmasks, zmasks=prob.zmasks, dtype=dt, device=local)
+        p.evaluate(prob.params[:16])
+        t0 = time.perf_counter()
+        E, G = p.evaluate(prob.params)
+        t = time.perf_counter() - t0
+        grads[dt] = G
+        res[dt] = {"vectors_per_s": len(prob.params) / t, "batch_ms": t * 1e3}
+        p.close()
+    res["c64_max_rel_grad_err"] = float(np.abs(grads["c64"] - grads["c128"]).max() /
+                                        max(1e-300, np.abs(grads["c128"]).max()))
+    return res
+
+
 class _DeviceView:
     """__cuda_array_interface__ over an engine-owned device buffer (for torch)."""
 
@@ -419,6 +495,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=15.0)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the per-gate GB/s sweep")
+    ap.add_argument("--no-vqe", action="store_true", help="skip the VQE adjoint-gradient leg")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     try:
