@@ -336,10 +336,24 @@ int  mlb_hea_num_parameters(const mlb_hea_t *h, uint32_t *out);
  * be NULL).  on_device = 1: all three are device pointers. */
 int  mlb_hea_evaluate(mlb_hea_t *h, size_t batch, const double *params, double *energies,
                       double *grads, int on_device);
-/* psi + lambda bytes allowed per sub-batch (0 = 80% of free device memory). */
+/* Device bytes an evaluation may hold in states: psi, lambda and checkpoints
+ * (0 = 80% of free device memory). */
 int  mlb_hea_set_memory_budget(mlb_hea_t *h, size_t bytes);
 int  mlb_hea_plan_stats(const mlb_hea_t *h, uint32_t *fwd_passes, uint32_t *lambda_passes,
                         uint32_t *bwd_passes);
+/* Checkpoints: the tape runs in segments of ceil(sqrt(L)) layers; with
+ * checkpoints the forward sweep keeps psi at each segment boundary and the
+ * backward sweep restores it there, so the uncompute by inverse gates never
+ * spans more than one segment (C - 1 extra states per vector for C
+ * segments).  mode 0 (default): checkpoints when they fit beside the whole
+ * batch in the budget; when memory is short they are dropped first, then the
+ * batch runs in sub-batches.  mode 1: always (sub-batches if needed);
+ * mode -1: never. */
+int  mlb_hea_set_checkpointing(mlb_hea_t *h, int mode);
+/* What the last mlb_hea_evaluate did: layers per segment, whether it kept
+ * checkpoints, and how many sub-batches it ran. */
+int  mlb_hea_last_eval_stats(const mlb_hea_t *h, uint32_t *segment_layers, int *checkpoints_used,
+                             size_t *sub_batches);
 const char *mlb_hea_last_error(void);
 
 /* ---- error text ---------------------------------------------------------- */

@@ -12,7 +12,14 @@
 //      produces E_b = <psi_b|lambda_b> (per-tile partials, fixed-order sum);
 //   4. backward tile passes over the reversed tape on (psi, lambda) with the
 //      per-parameter partials of Im<lambda|G|psi>; fixed-order sums.
-// Batches larger than the memory budget run in sub-batches.
+// Checkpoints: the tape is planned in segments of s = ceil(sqrt(L)) layers.
+// The forward sweep keeps psi at every segment boundary, and the backward
+// sweep restores psi from them instead of relying on the inverse gates
+// across the whole circuit, so the uncompute drift is bounded by one
+// segment (C - 1 extra states per vector for C segments).  Memory policy:
+// checkpoints when they fit next to the whole batch; when memory is short
+// they are dropped first (pure uncompute), then the batch runs in
+// sub-batches.  mlb_hea_set_checkpointing overrides the policy.
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -70,6 +77,15 @@ struct mlb_hea {
   std::vector<double> coeff;
   std::vector<TapeOp> tape;
   std::vector<GatePass> fwd, bwd;
+  // segments: fwd passes [fwd_seg[k], fwd_seg[k+1]) run segment k; bwd
+  // passes [bwd_seg[j], bwd_seg[j+1]) run segment C-1-j backwards
+  std::vector<size_t> fwd_seg, bwd_seg;
+  uint32_t seg_layers = 0;
+  int ckpt_mode = 0;         // 0 auto, 1 always, -1 never
+  void* ckpt = nullptr;
+  size_t ckpt_cap = 0;       // bytes
+  int last_ckpt = 0;
+  size_t last_chunks = 0;
   std::vector<TermPass> lam;
   cudaStream_t stream = nullptr;
   // device buffers
@@ -333,7 +349,7 @@ int upload_programs(mlb_hea* h) {
   return MLB_OK;
 }
 
-int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, double* h_G) {
+int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, double* h_G, bool use_ckpt) {
   const size_t dim = (size_t)1 << h->n;
   const size_t ab = h->dtype == MLB_C128 ? 16 : 8;
   int rc;
@@ -353,6 +369,17 @@ int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, do
     if (e != cudaSuccess) return cfail(e, "psi/lambda allocation");
     h->batch_cap = B;
   }
+  if (use_ckpt) {
+    const size_t need = (h->fwd_seg.size() - 2) * B * dim * ab;
+    if (h->ckpt_cap < need) {
+      if (h->ckpt) cudaFree(h->ckpt);
+      h->ckpt = nullptr;
+      h->ckpt_cap = 0;
+      cudaError_t e = cudaMalloc(&h->ckpt, need);
+      if (e != cudaSuccess) return cfail(e, "checkpoint allocation");
+      h->ckpt_cap = need;
+    }
+  }
   size_t max_slots_tiles = 1, max_tiles = 1;
   for (auto& gp : h->bwd) max_slots_tiles = std::max(max_slots_tiles, gp.P.tiles_per_state * B * (size_t)gp.P.num_slots);
   for (auto& tp : h->lam) max_tiles = std::max(max_tiles, tp.P.tiles_per_state * B);
@@ -362,12 +389,22 @@ int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, do
   // 2. forward
   // |0...0>: the tape itself starts with X on the hf_reference bits (vqe.c:1953-1959)
   if ((rc = launch_adj_init(h->dtype, h->psi, (int)h->n, B, 0, h->stream))) return hfail(rc, "init kernel");
-  for (auto& gp : h->fwd) {
-    AdjPass P = gp.P;
-    P.num_tiles = P.tiles_per_state * B;
-    if ((rc = launch_adj_gates(h->dtype, h->psi, nullptr, P, h->d_ops + gp.ops_off, h->d_cs, nullptr, false, false,
-                               h->num_sms, h->stream)))
-      return hfail(rc, "forward pass");
+  const size_t nseg = h->fwd_seg.size() - 1;
+  const size_t state_bytes = B * dim * ab;
+  for (size_t k = 0; k < nseg; k++) {
+    for (size_t i = h->fwd_seg[k]; i < h->fwd_seg[k + 1]; i++) {
+      const GatePass& gp = h->fwd[i];
+      AdjPass P = gp.P;
+      P.num_tiles = P.tiles_per_state * B;
+      if ((rc = launch_adj_gates(h->dtype, h->psi, nullptr, P, h->d_ops + gp.ops_off, h->d_cs, nullptr, false,
+                                 false, h->num_sms, h->stream)))
+        return hfail(rc, "forward pass");
+    }
+    if (use_ckpt && k + 1 < nseg) {
+      cudaError_t e = cudaMemcpyAsync((char*)h->ckpt + k * state_bytes, h->psi, state_bytes,
+                                      cudaMemcpyDeviceToDevice, h->stream);
+      if (e != cudaSuccess) return cfail(e, "checkpoint save");
+    }
   }
   // 3. lambda = H psi and the energies
   for (size_t k = 0; k < h->lam.size(); k++) {
@@ -382,7 +419,15 @@ int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, do
   }
   // 4. backward
   if (h_G) {
-    for (auto& gp : h->bwd) {
+    for (size_t j = 0; j < nseg; j++) {
+      const size_t k = nseg - 1 - j;  // segment swept backwards
+      if (use_ckpt && k + 1 < nseg) {  // psi at the end of segment k, as the forward sweep left it
+        cudaError_t e = cudaMemcpyAsync(h->psi, (char*)h->ckpt + k * state_bytes, state_bytes,
+                                        cudaMemcpyDeviceToDevice, h->stream);
+        if (e != cudaSuccess) return cfail(e, "checkpoint restore");
+      }
+    for (size_t i = h->bwd_seg[j]; i < h->bwd_seg[j + 1]; i++) {
+      const GatePass& gp = h->bwd[i];
       AdjPass P = gp.P;
       P.num_tiles = P.tiles_per_state * B;
       if ((rc = launch_adj_gates(h->dtype, h->psi, h->lamb, P, h->d_ops + gp.ops_off, h->d_cs, h->d_part, true,
@@ -392,6 +437,7 @@ int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, do
           (rc = launch_adj_reduce(h->d_part, P.tiles_per_state, P.num_slots, B, h->d_slots + gp.slots_off,
                                   (int)h->P, h->d_out + B, h->stream)))
         return hfail(rc, "gradient reduce");
+    }
     }
   }
   if (h_E) cudaMemcpyAsync(h_E, h->d_out, B * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
@@ -452,9 +498,24 @@ int mlb_hea_create(uint32_t n, uint32_t layers, uint64_t hf, size_t num_terms, c
     }
     for (uint32_t q = 0; q + 1 < n; q++) h->tape.push_back({ADJ_KIND_X, (int)q + 1, (int)q, -1});
   }
-  plan_gates(h, h->tape, false, h->fwd);
-  std::vector<TapeOp> rev(h->tape.rbegin(), h->tape.rend());
-  plan_gates(h, rev, true, h->bwd);
+  // segments of s = ceil(sqrt(L)) layers (the hf X prefix joins segment 0)
+  h->seg_layers = (uint32_t)std::ceil(std::sqrt((double)layers));
+  const size_t per_layer = 3 * (size_t)n - 1, prefix = h->tape.size() - per_layer * layers;
+  std::vector<size_t> cut{0};
+  for (uint32_t l = h->seg_layers; l < layers; l += h->seg_layers) cut.push_back(prefix + l * per_layer);
+  cut.push_back(h->tape.size());
+  h->fwd_seg.push_back(0);
+  for (size_t k = 0; k + 1 < cut.size(); k++) {
+    std::vector<TapeOp> sub(h->tape.begin() + cut[k], h->tape.begin() + cut[k + 1]);
+    plan_gates(h, sub, false, h->fwd);
+    h->fwd_seg.push_back(h->fwd.size());
+  }
+  h->bwd_seg.push_back(0);
+  for (size_t k = cut.size() - 1; k-- > 0;) {
+    std::vector<TapeOp> rev(h->tape.rend() - cut[k + 1], h->tape.rend() - cut[k]);
+    plan_gates(h, rev, true, h->bwd);
+    h->bwd_seg.push_back(h->bwd.size());
+  }
   plan_terms(h);
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete h;
@@ -473,8 +534,8 @@ void mlb_hea_free(mlb_hea_t* h) {
   if (!h) return;
   Guard g(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (void* p : {h->psi, h->lamb, (void*)h->d_cs, (void*)h->d_part, (void*)h->d_epart, (void*)h->d_ops,
-                  (void*)h->d_terms, (void*)h->d_slots, (void*)h->d_out})
+  for (void* p : {h->psi, h->lamb, h->ckpt, (void*)h->d_cs, (void*)h->d_part, (void*)h->d_epart,
+                  (void*)h->d_ops, (void*)h->d_terms, (void*)h->d_slots, (void*)h->d_out})
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -518,19 +579,26 @@ int mlb_hea_evaluate(mlb_hea_t* h, size_t batch, const double* params, double* e
   if (energies) hE.resize(batch);
   if (grads) hG.resize(batch * P);
   // sub-batches within the memory budget
+  const size_t sb = ((size_t)1 << h->n) * (h->dtype == MLB_C128 ? 16 : 8);  // one state
+  const size_t extra = h->fwd_seg.size() - 2;                                  // checkpoints per vector
   size_t budget = h->budget;
-  if (!budget) {
+  if (!budget) {  // 80 % of what is free, counting buffers this problem already holds
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
-    budget = (size_t)((fr + (h->batch_cap * ((size_t)2 << h->n) * (h->dtype == MLB_C128 ? 16 : 8))) * 0.8);
+    budget = (size_t)((fr + h->batch_cap * 2 * sb + h->ckpt_cap) * 0.8);
   }
-  const size_t per = ((size_t)2 << h->n) * (h->dtype == MLB_C128 ? 16 : 8);
+  // checkpoints when they fit with the whole batch (mode 1: always; -1: never)
+  bool use_ckpt = extra > 0 && grads != nullptr && h->ckpt_mode >= 0 &&
+                  (h->ckpt_mode == 1 || budget / ((2 + extra) * sb) >= batch);
+  const size_t per = (2 + (use_ckpt ? extra : 0)) * sb;
   size_t chunk = std::max<size_t>(1, budget / per);
   chunk = std::min(chunk, batch);
+  h->last_ckpt = use_ckpt ? 1 : 0;
+  h->last_chunks = (batch + chunk - 1) / chunk;
   for (size_t b0 = 0; b0 < batch; b0 += chunk) {
     const size_t nb = std::min(chunk, batch - b0);
     int rc = evaluate_chunk(h, nb, p_in + b0 * P, energies ? hE.data() + b0 : nullptr,
-                            grads ? hG.data() + b0 * P : nullptr);
+                            grads ? hG.data() + b0 * P : nullptr, use_ckpt);
     if (rc) return rc;
   }
   if (energies) {
@@ -541,6 +609,22 @@ int mlb_hea_evaluate(mlb_hea_t* h, size_t batch, const double* params, double* e
     if (on_device) cudaMemcpy(grads, hG.data(), batch * P * sizeof(double), cudaMemcpyHostToDevice);
     else std::memcpy(grads, hG.data(), batch * P * sizeof(double));
   }
+  return MLB_OK;
+}
+
+int mlb_hea_set_checkpointing(mlb_hea_t* h, int mode) {
+  if (!h) return hfail(MLB_ERR_INVALID_ARG, "null problem");
+  if (mode < -1 || mode > 1) return hfail(MLB_ERR_INVALID_ARG, "mode must be -1, 0 or 1");
+  h->ckpt_mode = mode;
+  return MLB_OK;
+}
+
+int mlb_hea_last_eval_stats(const mlb_hea_t* h, uint32_t* segment_layers, int* checkpoints_used,
+                            size_t* sub_batches) {
+  if (!h) return hfail(MLB_ERR_INVALID_ARG, "null problem");
+  if (segment_layers) *segment_layers = h->seg_layers;
+  if (checkpoints_used) *checkpoints_used = h->last_ckpt;
+  if (sub_batches) *sub_batches = h->last_chunks;
   return MLB_OK;
 }
 

@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import MlbError, load
+from ._lib import MlbError, check, load
 
 
 def pauli_masks(paulis):
@@ -70,6 +70,18 @@ class HEAProblem:
 
     def set_memory_budget(self, nbytes: int) -> None:
         self._lib.mlb_hea_set_memory_budget(self._h, int(nbytes))
+
+    def set_checkpointing(self, mode: str = "auto") -> None:
+        """'auto' (checkpoints every ceil(sqrt(L)) layers when they fit beside
+        the whole batch), 'always' or 'never'."""
+        code = {"auto": 0, "always": 1, "never": -1}[mode]
+        check(self._lib.mlb_hea_set_checkpointing(self._h, code), "mlb_hea_set_checkpointing")
+
+    def last_eval_stats(self) -> dict:
+        seg, used, chunks = C.c_uint32(), C.c_int(), C.c_size_t()
+        check(self._lib.mlb_hea_last_eval_stats(self._h, C.byref(seg), C.byref(used), C.byref(chunks)),
+              "mlb_hea_last_eval_stats")
+        return {"segment_layers": seg.value, "checkpoints": bool(used.value), "sub_batches": chunks.value}
 
     def plan_stats(self):
         f, l, b = C.c_uint32(), C.c_uint32(), C.c_uint32()

@@ -145,3 +145,39 @@ def test_dropin_moonlab_vqe_gradient_on_reference_solver(gpu):
     assert lib.moonlab_vqe_gradient(None, _dp(pp), _dp(g), P) == -1
     assert lib.moonlab_vqe_gradient(s.solver, _dp(pp), _dp(g), P - 1) == -2
     s.close()
+
+
+def test_checkpointed_backward_sweep(gpu):
+    """Checkpoints every ceil(sqrt(L)) layers give the same gradients (the
+    restored psi equals the uncomputed one to rounding), and the memory
+    policy drops them before splitting the batch."""
+    paulis, coeffs, params, hf = random_problem(12, 9, 24, 31)
+    prob = HEAProblem(12, 9, coeffs, paulis=paulis, hf_reference=hf)
+    prob.set_checkpointing("always")
+    E1, G1 = prob.evaluate(params)
+    st = prob.last_eval_stats()
+    assert st["checkpoints"] and st["segment_layers"] == 3 and st["sub_batches"] == 1
+    prob.set_checkpointing("never")
+    E2, G2 = prob.evaluate(params)
+    assert not prob.last_eval_stats()["checkpoints"]
+    assert np.array_equal(E1, E2)
+    assert np.abs(G1 - G2).max() < 1e-12
+    for k in range(len(params)):
+        _, g_ref = port_energy_grad(12, 9, hf, paulis, coeffs, params[k])
+        assert np.abs(G1[k] - g_ref).max() < 1e-11
+    # auto: a budget for psi + lambda of all 3 vectors but not their 2 checkpoints each
+    state = 16 << 12
+    prob.set_checkpointing("auto")
+    prob.set_memory_budget(3 * 2 * state + state)
+    _, G3 = prob.evaluate(params)
+    st = prob.last_eval_stats()
+    assert not st["checkpoints"] and st["sub_batches"] == 1
+    prob.set_memory_budget(3 * 4 * state)
+    _, G4 = prob.evaluate(params)
+    assert prob.last_eval_stats()["checkpoints"]
+    prob.set_memory_budget(2 * state)  # one vector at a time, no room for checkpoints
+    _, G5 = prob.evaluate(params)
+    st = prob.last_eval_stats()
+    assert not st["checkpoints"] and st["sub_batches"] == 3
+    for G in (G3, G4, G5):
+        assert np.abs(G - G1).max() < 1e-12
