@@ -237,7 +237,10 @@ int  mlb_job_run(const mlb_job_desc_t *desc, const mlb_gate_t *gates, size_t num
  * uniforms from xorshift64(rng_seed), each shot measurement_all_qubits(u) on
  * the circuit's output state (rng_seed 0 takes the clock).  Results do not
  * depend on the other requests in flight.  Times in mlb_request_info_t are
- * seconds since the server was created.  mlb_server_wait blocks up to
+ * seconds since the server was created.  Small requests (<= 12 qubits
+ * complex128, <= 13 complex64) skip the state pool: the waiting ones of a
+ * dtype run together in one launch, one thread block per circuit with its
+ * state in shared memory.  mlb_server_wait blocks up to
  * timeout_ms (< 0: no limit; MLB_ERR_TIMEOUT when it runs out), copies the
  * outcomes (capacity >= num_shots), releases the ticket and returns the
  * request's status.  mlb_server_destroy cancels requests not yet admitted
@@ -263,6 +266,7 @@ typedef struct {
 typedef struct {
     uint64_t submitted, completed, failed, pending, running, peak_running;
     uint64_t reserved_bytes, peak_reserved_bytes, budget_bytes;
+    uint64_t small_batches, small_requests;  /* size-class launches and the requests they ran */
 } mlb_server_stats_t;
 int  mlb_server_create(int device, size_t hbm_budget_bytes, int num_workers, mlb_server_t **out);
 int  mlb_server_submit(mlb_server_t *s, const mlb_request_t *req, uint64_t *ticket);

@@ -1127,6 +1127,30 @@ int mlb_run_gates(mlb_state_t* s, const mlb_gate_t* gates, size_t num) {
   return mlb_apply_ops(s, ops.data(), cnt);
 }
 
+}  // extern "C"
+
+int mlb::prepare_ops(const mlb_gate_t* gates, size_t num, uint32_t n, std::vector<mlb_op_t>& out) {
+  size_t cnt = 0;
+  int rc = mlb_gates_to_ops(gates, num, n, nullptr, &cnt);
+  if (rc) return rc;
+  std::vector<mlb_op_t> raw(cnt);
+  rc = mlb_gates_to_ops(gates, num, n, raw.data(), &cnt);
+  if (rc) return rc;
+  mlb_state probe;  // host-side only: validation needs n
+  probe.n = n;
+  std::vector<mlb_op_t> q;
+  q.reserve(cnt);
+  for (size_t i = 0; i < cnt; i++) {
+    rc = validate(&probe, raw[i]);
+    if (rc) return rc;
+    q.push_back(canonical(raw[i]));
+  }
+  out = fuse_1q_runs(q, n);
+  return MLB_OK;
+}
+
+extern "C" {
+
 int mlb_plan_ops(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fuse1q,
                  mlb_flush_stats_t* out) {
   if ((!ops && num) || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");

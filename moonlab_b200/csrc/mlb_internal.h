@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "moonlab_b200.h"
@@ -174,6 +175,22 @@ struct FusedPassDev {
   uint32_t block_begin;
   uint32_t num_blocks;
 };
+// ---- small circuits in one launch (kernels_small.cu; the serving path) ----
+// One request per item: ops[ops_off .. ops_off + num_ops) on an n-qubit
+// state from |0...0>, then shots outcomes for uniforms[uni_off ..] written
+// to outcomes[out_off ..].
+struct SmallItem {
+  uint64_t ops_off, uni_off, out_off;
+  uint32_t num_ops, n, shots, pad;
+};
+int small_max_qubits(int dtype);  // 12 (complex128) / 13 (complex64): the state fits a CTA
+int launch_small_circuits(int dtype, const SmallItem* d_items, int num_items, const mlb_op_t* d_ops,
+                          const double* d_uniforms, unsigned long long* d_outcomes, uint32_t nmax,
+                          int num_sms, cudaStream_t stream);
+// Gate records -> validated, canonical ops with 1q runs fused (what a flush
+// of mlb_run_gates would plan).
+int prepare_ops(const mlb_gate_t* gates, size_t num_gates, uint32_t n, std::vector<mlb_op_t>& out);
+
 // d_err: device word set non-zero if a tensor-core completion wait ran out.
 int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,
                       const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream);

@@ -17,6 +17,12 @@
 // result does not depend on what else runs: its kernels read and write only
 // its own state and every reduction has a fixed order.
 //
+// Small requests (<= 12 qubits complex128, <= 13 complex64) need no pooled
+// state: a worker that admits one also takes every other small request of
+// the same dtype waiting in the queue and runs them all in one launch, one
+// CTA per circuit with the state in shared memory (kernels_small.cu), on its
+// own stream.
+//
 // A large state's tile passes fill every SM for the length of a pass, so
 // each pooled state gets its own stream with a priority by size class
 // (smaller states higher): whenever SMs free up, the block scheduler
@@ -45,6 +51,7 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr size_t kStateOverhead = 1 << 20;  // per-state scratch and sampling buffers, bounded
+constexpr size_t kMaxSmallBatch = 1024;     // small requests per launch
 
 struct Request {
   uint64_t ticket = 0;
@@ -101,10 +108,17 @@ struct mlb_server {
   // state when one fits; otherwise the request's bytes are reserved and
   // *evict lists idle states to free first.  First fit in arrival order,
   // except that a request waiting longer than starvation_s blocks later ones.
+  static bool is_small(const Request* r) { return (int)r->n <= mlb::small_max_qubits(r->dtype); }
+
   Request* pick(mlb_state_t** state, std::vector<mlb_state_t*>* evict) {
     const double t = now();
     for (auto it = pending.begin(); it != pending.end(); ++it) {
       Request* r = *it;
+      if (is_small(r)) {  // no device state of its own
+        *state = nullptr;
+        pending.erase(it);
+        return r;
+      }
       auto key = std::make_pair(r->n, r->dtype);
       auto pit = idle.find(key);
       if (pit != idle.end() && !pit->second.empty()) {
@@ -183,15 +197,139 @@ struct mlb_server {
     if (st) cudaStreamDestroy(st);
   }
 
+  // Device buffers of one worker's small batches (grow only).
+  struct SmallBufs {
+    cudaStream_t stream = nullptr;
+    mlb::SmallItem* items = nullptr;
+    mlb_op_t* ops = nullptr;
+    double* uni = nullptr;
+    unsigned long long* out = nullptr;
+    size_t cap_items = 0, cap_ops = 0, cap_uni = 0, cap_out = 0;
+  };
+
+  template <typename T>
+  static int grow(T*& p, size_t& cap, size_t n) {
+    if (n <= cap) return MLB_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max(n, cap * 2);
+    if (cudaMalloc((void**)&p, want * sizeof(T)) != cudaSuccess) {
+      cudaGetLastError();
+      return MLB_ERR_OUT_OF_MEMORY;
+    }
+    cap = want;
+    return MLB_OK;
+  }
+
+  // Runs a batch of small requests in one launch; sets each one's status.
+  void run_small(std::vector<Request*>& batch, SmallBufs& B) {
+    const int dtype = batch[0]->dtype;
+    std::vector<mlb::SmallItem> items;
+    std::vector<mlb_op_t> ops;
+    std::vector<double> uni;
+    std::vector<Request*> live;
+    uint32_t nmax = 1;
+    for (Request* r : batch) {
+      std::vector<mlb_op_t> o;
+      const int rc = mlb::prepare_ops(r->gates.data(), r->gates.size(), r->n, o);
+      if (rc) {
+        r->status = rc;
+        continue;
+      }
+      mlb::SmallItem it{};
+      it.ops_off = ops.size();
+      it.num_ops = (uint32_t)o.size();
+      it.n = r->n;
+      it.shots = r->shots;
+      it.uni_off = uni.size();
+      it.out_off = uni.size();
+      ops.insert(ops.end(), o.begin(), o.end());
+      uint64_t seed = r->seed ? r->seed : ((uint64_t)std::time(nullptr) ^ 0x9e3779b97f4a7c15ULL);
+      for (uint32_t k = 0; k < r->shots; k++) uni.push_back((double)(xorshift64(seed) >> 11) / (double)(1ULL << 53));
+      items.push_back(it);
+      live.push_back(r);
+      nmax = std::max(nmax, r->n);
+    }
+    if (live.empty()) return;
+    int rc = MLB_OK;
+    if (!B.stream && cudaStreamCreateWithPriority(&B.stream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess)
+      rc = MLB_ERR_DRIVER;
+    if (!rc) rc = grow(B.items, B.cap_items, items.size());
+    if (!rc) rc = grow(B.ops, B.cap_ops, std::max<size_t>(1, ops.size()));
+    if (!rc) rc = grow(B.uni, B.cap_uni, std::max<size_t>(1, uni.size()));
+    if (!rc) rc = grow(B.out, B.cap_out, std::max<size_t>(1, uni.size()));
+    std::vector<unsigned long long> out(uni.size());
+    if (!rc) {
+      cudaMemcpyAsync(B.items, items.data(), items.size() * sizeof(mlb::SmallItem), cudaMemcpyHostToDevice, B.stream);
+      if (!ops.empty())
+        cudaMemcpyAsync(B.ops, ops.data(), ops.size() * sizeof(mlb_op_t), cudaMemcpyHostToDevice, B.stream);
+      if (!uni.empty())
+        cudaMemcpyAsync(B.uni, uni.data(), uni.size() * sizeof(double), cudaMemcpyHostToDevice, B.stream);
+      int sms = 148;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+      rc = mlb::launch_small_circuits(dtype, B.items, (int)items.size(), B.ops, B.uni, B.out, nmax, sms, B.stream);
+      if (!rc && !uni.empty())
+        cudaMemcpyAsync(out.data(), B.out, out.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                        B.stream);
+      if (!rc && cudaStreamSynchronize(B.stream) != cudaSuccess) rc = MLB_ERR_DRIVER;
+    }
+    for (size_t i = 0; i < live.size(); i++) {
+      Request* r = live[i];
+      if (!rc) r->outcomes.assign(out.begin() + items[i].out_off, out.begin() + items[i].out_off + r->shots);
+      r->status = rc;
+    }
+  }
+
   void worker() {
     cudaSetDevice(device);
+    SmallBufs sbufs;
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
       mlb_state_t* state = nullptr;
       std::vector<mlb_state_t*> evict;
       Request* r = nullptr;
       while (!stopping && !(r = pick(&state, &evict))) cv_work.wait(lk);
-      if (!r) return;  // stopping
+      if (!r) {  // stopping
+        lk.unlock();
+        for (void* p : {(void*)sbufs.items, (void*)sbufs.ops, (void*)sbufs.uni, (void*)sbufs.out})
+          if (p) cudaFree(p);
+        if (sbufs.stream) cudaStreamDestroy(sbufs.stream);
+        return;
+      }
+      if (is_small(r)) {
+        std::vector<Request*> batch{r};
+        for (auto it = pending.begin(); it != pending.end() && batch.size() < kMaxSmallBatch;) {
+          if (is_small(*it) && (*it)->dtype == r->dtype) {
+            batch.push_back(*it);
+            it = pending.erase(it);
+          } else {
+            ++it;
+          }
+        }
+        const double ta = now();
+        for (Request* q : batch) {
+          q->status = 2;
+          q->t_admit = ta;
+        }
+        running += (int)batch.size();
+        st.peak_running = std::max<uint64_t>(st.peak_running, (uint64_t)running);
+        st.small_batches++;
+        st.small_requests += batch.size();
+        lk.unlock();
+        run_small(batch, sbufs);
+        lk.lock();
+        running -= (int)batch.size();
+        const double td = now();
+        for (Request* q : batch) {
+          q->t_done = td;
+          if (q->status) st.failed++;
+          st.completed++;
+        }
+        cv_done.notify_all();
+        cv_work.notify_all();
+        continue;
+      }
       r->status = 2;
       r->t_admit = now();
       running++;

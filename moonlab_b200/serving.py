@@ -36,7 +36,7 @@ class MlbRequestInfo(C.Structure):
 class MlbServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "failed", "pending", "running",
                                           "peak_running", "reserved_bytes", "peak_reserved_bytes",
-                                          "budget_bytes")]
+                                          "budget_bytes", "small_batches", "small_requests")]
 
 
 _SIGS = {

@@ -100,3 +100,38 @@ def test_budget_errors_and_timeouts(gpu):
         out, info = s.wait(t2)
         assert info["status"] == 0 and len(out) == 1
         assert s.stats()["completed"] == 2
+
+
+@pytest.mark.gpu
+def test_small_requests_share_launches(gpu):
+    """Small circuits (<= 12 qubits c128, <= 13 c64) run many per launch;
+    each one's outcomes equal its run alone and, for complex128, the
+    oracle's moonlab_qgtl_execute bit for bit."""
+    from moonlab_b200.serving import Server
+    from test_fused_plan import mixed_circuit
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(150):
+        dt = int(rng.integers(0, 2))
+        n = int(rng.integers(3, 13 if dt == 0 else 14))
+        g = mixed_circuit(n, int(rng.integers(2, 12)), 100 + i) if n >= 4 else brickwork(n, 6, 100 + i, 2)
+        reqs.append((n, g, int(rng.integers(1, 700)), int(rng.integers(1, 2**62)), "c64" if dt else "c128"))
+    alone = []
+    with Server(workers=1) as s:
+        for n, g, shots, seed, dt in reqs:
+            alone.append(s.wait(s.submit(n, g, shots, seed, dt))[0])
+    with Server(workers=2) as s:
+        tickets = [s.submit(*r) for r in reqs]
+        mixed = [s.wait(t)[0] for t in tickets]
+        st = s.stats()
+    assert st["small_requests"] == len(reqs)
+    assert st["small_batches"] < len(reqs)
+    for a, b in zip(alone, mixed):
+        assert np.array_equal(a, b)
+    for (n, g, shots, seed, dt), out in zip(reqs, mixed):
+        if dt == "c128":
+            want = np.empty(shots, dtype=np.uint64)
+            sv = B.to_svo(g)
+            assert B.port().svo_qgtl_execute(n, sv, len(sv), shots, seed,
+                                              want.ctypes.data_as(C.POINTER(C.c_uint64)), None) == 0
+            assert np.array_equal(out, want)
