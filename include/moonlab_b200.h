@@ -267,6 +267,7 @@ typedef struct {
     uint64_t submitted, completed, failed, pending, running, peak_running;
     uint64_t reserved_bytes, peak_reserved_bytes, budget_bytes;
     uint64_t small_batches, small_requests;  /* size-class launches and the requests they ran */
+    uint64_t plan_cache_hits;                /* requests whose plan came from a state's cache */
 } mlb_server_stats_t;
 int  mlb_server_create(int device, size_t hbm_budget_bytes, int num_workers, mlb_server_t **out);
 int  mlb_server_submit(mlb_server_t *s, const mlb_request_t *req, uint64_t *ticket);
@@ -284,8 +285,17 @@ typedef struct {
     uint64_t kernel_launches;
     uint64_t segments;       /* shared-memory register-group round trips over all passes */
     double   gpu_ms;         /* device time of the flush's kernels (timing enabled), else 0 */
+    uint64_t plan_cache_hit; /* 1 when the plan came from the state's plan cache */
 } mlb_flush_stats_t;
 int  mlb_last_flush_stats(mlb_state_t *s, mlb_flush_stats_t *out);
+/* Plan cache for repeated circuit shapes (tiled mode): up to `entries` plans
+ * are kept per state, keyed by the shape of the flushed ops (kinds, qubits,
+ * controls, real or complex 1-qubit matrices -- not the angles).  A flush
+ * whose shape was seen before skips planning: it patches this circuit's
+ * matrices into the cached op program and replays the passes' launches as
+ * one CUDA graph (captured at the shape's first replay).  Results are
+ * identical with and without the cache.  0 entries (default) = off. */
+int  mlb_state_set_plan_cache(mlb_state_t *s, size_t entries);
 /* Record CUDA events around each flush's kernels on the state's stream;
  * mlb_last_flush_stats then reports their elapsed device time (synchronizes). */
 int  mlb_state_set_timing(mlb_state_t *s, int enable);

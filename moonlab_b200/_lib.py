@@ -40,7 +40,7 @@ class MlbGate(C.Structure):
 class MlbFlushStats(C.Structure):
     _fields_ = [("passes", C.c_uint64), ("ops", C.c_uint64), ("dense_blocks", C.c_uint64),
                 ("bytes_moved", C.c_uint64), ("kernel_launches", C.c_uint64), ("segments", C.c_uint64),
-                ("gpu_ms", C.c_double)]
+                ("gpu_ms", C.c_double), ("plan_cache_hit", C.c_uint64)]
 
 
 class MlbJobDesc(C.Structure):
@@ -125,6 +125,7 @@ _SIGS = {
     "mlb_run_gates": (C.c_int, [C.c_void_p, C.POINTER(MlbGate), C.c_size_t]),
     "mlb_last_flush_stats": (C.c_int, [C.c_void_p, C.POINTER(MlbFlushStats)]),
     "mlb_state_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "mlb_state_set_plan_cache": (C.c_int, [C.c_void_p, C.c_size_t]),
     "mlb_plan_ops": (C.c_int, [C.POINTER(MlbOp), C.c_size_t, C.c_uint32, C.c_int, C.c_int,
                                C.POINTER(MlbFlushStats)]),
     "mlb_total_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),

@@ -109,6 +109,21 @@ struct mlb_state {
   int* d_ferr = nullptr;
   int* h_ferr = nullptr;
   bool ferr_pending = false;
+  // plan cache for repeated circuit shapes (tiled mode; 0 entries = off)
+  struct PlanEntry {
+    std::vector<uint64_t> shape;              // the fused ops' shape words
+    std::vector<DevOp> dops;                  // op program; matrices patched per use
+    std::vector<int> src;                     // fused-op index of every dop
+    std::vector<DevSegment> segs;
+    std::vector<mlb::plan::PlannedPass> passes;
+    cudaGraphExec_t exec = nullptr;           // the passes' launches, captured once
+    void* graph_dplan = nullptr;              // d_plan the graph was captured with
+    uint64_t last_use = 0;
+  };
+  std::vector<PlanEntry> plan_cache;
+  size_t plan_cache_cap = 0;
+  uint64_t plan_clock = 0;
+  uint64_t plan_hits = 0, plan_misses = 0;
 };
 
 namespace {
@@ -384,6 +399,27 @@ int upload_plan(mlb_state* s, const void* host, size_t bytes) {
   return MLB_OK;
 }
 
+// Shape of a planned op list: everything the planner's decisions depend on
+// (kind, qubits, controls, and whether a 1-qubit matrix is real), but not
+// the matrix values.  Equal shapes plan identically.
+std::vector<uint64_t> plan_shape(const mlb_state* s, const std::vector<mlb_op_t>& ops) {
+  std::vector<uint64_t> w;
+  w.reserve(2 * ops.size() + 1);
+  w.push_back((uint64_t)s->n | (uint64_t)s->dtype << 8);
+  for (const auto& o : ops) {
+    uint64_t real = 0;
+    if (o.kind == MLB_OP_1Q) {
+      real = 1;
+      for (int t = 1; t < 8; t += 2)
+        if (o.m[t] != 0.0) real = 0;
+    }
+    w.push_back((uint64_t)(uint32_t)o.kind | (uint64_t)(uint8_t)o.target << 8 |
+                (uint64_t)(uint8_t)o.target2 << 16 | real << 24);
+    w.push_back(o.cmask);
+  }
+  return w;
+}
+
 // Fused complex64 path: dense <= 5-qubit blocks on the tensor cores.
 int flush_fused(mlb_state* s, const std::vector<mlb_op_t>& ops) {
   fused::Plan P;
@@ -457,30 +493,102 @@ int flush_impl(mlb_state* s) {
   std::vector<mlb_op_t> ops = s->fuse1q ? fuse_1q_runs(s->queue, s->n) : s->queue;
   s->queue.clear();
   if (s->mode == MLB_EXEC_FUSED) return flush_fused(s, ops);
-  Planner pl{s->n, s->dtype, geo(s->dtype)};
-  pl.plan(ops);
+  // the plan: from the cache when this shape ran before, else planned now
+  mlb_state::PlanEntry local;
+  mlb_state::PlanEntry* E = &local;
+  bool hit = false;
+  std::vector<uint64_t> shape;
+  if (s->plan_cache_cap) {
+    shape = plan_shape(s, ops);
+    for (auto& e : s->plan_cache)
+      if (e.shape == shape) {
+        E = &e;
+        hit = true;
+        break;
+      }
+  }
+  if (!hit) {
+    Planner pl{s->n, s->dtype, geo(s->dtype)};
+    pl.plan(ops);
+    local.dops = std::move(pl.dops);
+    local.src = std::move(pl.dop_src);
+    local.segs = std::move(pl.segs);
+    local.passes = std::move(pl.passes);
+    if (s->plan_cache_cap) {
+      local.shape = std::move(shape);
+      if (s->plan_cache.size() >= s->plan_cache_cap) {  // evict the least recently used
+        auto lru = std::min_element(s->plan_cache.begin(), s->plan_cache.end(),
+                                    [](const auto& a, const auto& b) { return a.last_use < b.last_use; });
+        if (lru->exec) cudaGraphExecDestroy(lru->exec);
+        s->plan_cache.erase(lru);
+      }
+      s->plan_cache.push_back(std::move(local));
+      E = &s->plan_cache.back();
+    }
+    s->plan_misses++;
+  } else {
+    for (size_t i = 0; i < E->dops.size(); i++)  // this circuit's matrices into the cached program
+      std::memcpy(E->dops[i].m, ops[E->src[i]].m, sizeof(E->dops[i].m));
+    s->plan_hits++;
+  }
+  E->last_use = ++s->plan_clock;
   // one upload: ops then segments
-  const size_t ob = pl.dops.size() * sizeof(DevOp);
-  const size_t sb = pl.segs.size() * sizeof(DevSegment);
+  const size_t ob = E->dops.size() * sizeof(DevOp);
+  const size_t sb = E->segs.size() * sizeof(DevSegment);
   std::vector<unsigned char> blob(ob + sb + 16);
-  std::memcpy(blob.data(), pl.dops.data(), ob);
+  std::memcpy(blob.data(), E->dops.data(), ob);
   size_t soff = (ob + 15) & ~(size_t)15;
-  std::memcpy(blob.data() + soff, pl.segs.data(), sb);
+  std::memcpy(blob.data() + soff, E->segs.data(), sb);
   int rc = upload_plan(s, blob.data(), soff + sb);
   if (rc) return rc;
   const DevOp* d_ops = reinterpret_cast<const DevOp*>(s->d_plan);
   const DevSegment* d_segs = reinterpret_cast<const DevSegment*>((unsigned char*)s->d_plan + soff);
+  auto launch_passes = [&]() -> int {
+    for (const auto& pp : E->passes) {
+      int r = launch_tile_pass(s->dtype, s->amp, pp.pass, d_segs + pp.seg_begin, d_ops, nullptr, s->num_sms,
+                               s->stream);
+      if (r) return r;
+    }
+    return MLB_OK;
+  };
   if (s->timing) cudaEventRecord(s->t0, s->stream);
-  for (const auto& pp : pl.passes) {
-    rc = launch_tile_pass(s->dtype, s->amp, pp.pass, d_segs + pp.seg_begin, d_ops, nullptr, s->num_sms,
-                          s->stream);
-    if (rc) return fail(rc, "tile pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-    st.passes++;
-    st.kernel_launches++;
-    st.bytes_moved += 2 * ab * dim;
+  if (s->plan_cache_cap && E != &local) {
+    // replay the captured launches (capture once per plan buffer)
+    if (E->exec && E->graph_dplan != s->d_plan) {
+      cudaGraphExecDestroy(E->exec);
+      E->exec = nullptr;
+    }
+    if (!E->exec) {
+      prepare_tile_launch(s->dtype);  // function attributes before capture
+      cudaGraph_t g = nullptr;
+      bool ok = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        const int lr = launch_passes();
+        ok = cudaStreamEndCapture(s->stream, &g) == cudaSuccess && lr == MLB_OK && g;
+        if (ok) ok = cudaGraphInstantiate(&E->exec, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+      }
+      if (!ok) {
+        cudaGetLastError();
+        E->exec = nullptr;
+      }
+      E->graph_dplan = s->d_plan;
+    }
+    if (E->exec) {
+      if (cudaGraphLaunch(E->exec, s->stream) != cudaSuccess)
+        return fail(MLB_ERR_DRIVER, "graph launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    } else if ((rc = launch_passes())) {
+      return fail(rc, "tile pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+  } else if ((rc = launch_passes())) {
+    return fail(rc, "tile pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
+  st.passes = E->passes.size();
+  st.kernel_launches = E->passes.size();
+  st.bytes_moved = E->passes.size() * 2 * ab * dim;
   st.ops = ops.size();
-  st.segments = pl.segs.size();
+  st.segments = E->segs.size();
+  st.plan_cache_hit = hit ? 1 : 0;
   if (s->timing) {
     cudaEventRecord(s->t1, s->stream);
     s->timed_pending = true;
@@ -592,6 +700,8 @@ void mlb_state_free(mlb_state_t* s) {
   if (s->amp) cudaFree(s->amp);
   if (s->d_scratch) cudaFree(s->d_scratch);
   if (s->d_plan) cudaFree(s->d_plan);
+  for (auto& e : s->plan_cache)
+    if (e.exec) cudaGraphExecDestroy(e.exec);
   if (s->d_ferr) cudaFree(s->d_ferr);
   if (s->h_ferr) cudaFreeHost(s->h_ferr);
   if (s->h_plan) cudaFreeHost(s->h_plan);
@@ -647,6 +757,22 @@ int mlb_state_stream(const mlb_state_t* s, void** out) {
   *out = (void*)s->stream;
   return MLB_OK;
 }
+int mlb_state_set_plan_cache(mlb_state_t* s, size_t entries) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);
+  if (rc) return rc;
+  if (entries < s->plan_cache.size()) {
+    rc = sync_stream(s);  // graphs may still be running
+    if (rc) return rc;
+    for (auto& e : s->plan_cache)
+      if (e.exec) cudaGraphExecDestroy(e.exec);
+    s->plan_cache.clear();
+  }
+  s->plan_cache_cap = entries;
+  return MLB_OK;
+}
+
 int mlb_state_set_exec_mode(mlb_state_t* s, int mode) {
   if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
   if (mode != MLB_EXEC_TILED && mode != MLB_EXEC_EAGER && mode != MLB_EXEC_FUSED)

@@ -365,14 +365,11 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   }
 }
 
+// The shared-memory opt-in is a per-device function attribute; set it once
+// per device (threads may race here, and setting it twice is harmless).
 template <typename Real>
-int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, const DevOp* d_ops,
-                  int num_sms, cudaStream_t stream) {
+void prepare_tile_t() {
   using A = typename Cplx<Real>::T;
-  constexpr int NT = TileCfg<Real>::NT;
-  const size_t smem = sizeof(A) << (pass.L + pass.H);
-  // The shared-memory opt-in is a per-device function attribute; set it once
-  // per device (threads may race here, and setting it twice is harmless).
   static std::atomic<uint64_t> attr_set_mask{0};
   const size_t max_smem = sizeof(A) << TileCfg<Real>::TB;
   int dev = 0;
@@ -382,6 +379,15 @@ int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, cons
     cudaFuncSetAttribute(k_tile<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
     attr_set_mask.fetch_or(bit, std::memory_order_release);
   }
+}
+
+template <typename Real>
+int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, const DevOp* d_ops,
+                  int num_sms, cudaStream_t stream) {
+  using A = typename Cplx<Real>::T;
+  constexpr int NT = TileCfg<Real>::NT;
+  const size_t smem = sizeof(A) << (pass.L + pass.H);
+  prepare_tile_t<Real>();
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<Real>, NT, smem);
   if (per_sm < 1) per_sm = 1;
@@ -393,6 +399,11 @@ int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, cons
 }
 
 }  // namespace
+
+void prepare_tile_launch(int dtype) {
+  if (dtype == MLB_C128) prepare_tile_t<double>();
+  else prepare_tile_t<float>();
+}
 
 int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment* d_segs,
                      const DevOp* d_ops, const float2* d_mats, int num_sms, cudaStream_t stream) {

@@ -118,6 +118,9 @@ int launch_adj_reduce(const double* d_partials, uint64_t tiles_per_state, int nu
 // Kernel launchers (kernels_*.cu).  All asynchronous on `stream`.
 int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment* d_segs,
                      const DevOp* d_ops, const float2* d_mats, int num_sms, cudaStream_t stream);
+// Sets the tile kernel's function attributes on the current device (done
+// lazily by launch_tile_pass; called before a stream capture).
+void prepare_tile_launch(int dtype);
 int launch_gate(int dtype, void* amp, int n, const mlb_op_t& op, cudaStream_t stream);
 int launch_init_zero(int dtype, void* amp, int n, cudaStream_t stream);
 int launch_convert(int dst_dtype, void* dst, int src_dtype, const void* src, uint64_t dim,

@@ -55,6 +55,7 @@ struct Planner {
   std::vector<PlannedPass> passes;
   std::vector<DevSegment> segs;
   std::vector<DevOp> dops;
+  std::vector<int> dop_src;  // index into the planned ops of every entry of dops
 
   // Choose the ops of one pass from `rem` (indices into ops), program order.
   // Returns taken indices; fills high mask.
@@ -233,6 +234,7 @@ struct Planner {
         d.lt = local_of[o.target];
         d.k = local_of[o.target2];
         dops.push_back(d);
+        dop_src.push_back(taken[i]);
         sg.op_end = (int)dops.size();
         segs.push_back(sg);
         i++;
@@ -302,6 +304,7 @@ struct Planner {
           }
         }
         dops.push_back(d);
+        dop_src.push_back(taken[k]);
       }
       sg.op_end = (int)dops.size();
       segs.push_back(sg);

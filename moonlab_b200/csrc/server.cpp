@@ -23,6 +23,10 @@
 // CTA per circuit with the state in shared memory (kernels_small.cu), on its
 // own stream.
 //
+// Pooled states keep a plan cache: a request whose circuit shape (gate
+// kinds and qubits, not angles) ran before on that state skips planning and
+// replays the passes' launches as one CUDA graph.
+//
 // A large state's tile passes fill every SM for the length of a pass, so
 // each pooled state gets its own stream with a priority by size class
 // (smaller states higher): whenever SMs free up, the block scheduler
@@ -171,6 +175,7 @@ struct mlb_server {
     cudaStream_t st = nullptr;
     cudaError_t e = cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, priority(n));
     if (e == cudaSuccess) rc = mlb_state_set_stream(*out, (void*)st);
+    if (e == cudaSuccess && !rc) rc = mlb_state_set_plan_cache(*out, 8);  // repeated circuit shapes
     if (e != cudaSuccess || rc) {
       if (st) cudaStreamDestroy(st);
       mlb_state_free(*out);
@@ -351,6 +356,11 @@ struct mlb_server {
       } else if (!rc) {
         rc = mlb_synchronize(state);
       }
+      uint64_t hit = 0;
+      if (!rc) {
+        mlb_flush_stats_t fs{};
+        if (mlb_last_flush_stats(state, &fs) == MLB_OK) hit = fs.plan_cache_hit;
+      }
       if (rc && state) {  // do not pool a state in an unknown condition
         free_state(state);
         state = nullptr;
@@ -367,6 +377,7 @@ struct mlb_server {
       r->t_done = now();
       if (rc) st.failed++;
       st.completed++;
+      st.plan_cache_hits += hit;
       cv_done.notify_all();
       cv_work.notify_all();
     }

@@ -36,7 +36,8 @@ class MlbRequestInfo(C.Structure):
 class MlbServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "failed", "pending", "running",
                                           "peak_running", "reserved_bytes", "peak_reserved_bytes",
-                                          "budget_bytes", "small_batches", "small_requests")]
+                                          "budget_bytes", "small_batches", "small_requests",
+                                          "plan_cache_hits")]
 
 
 _SIGS = {

@@ -104,6 +104,9 @@ class StateVector:
         check(self._lib.mlb_last_flush_stats(self._h, C.byref(st)), "mlb_last_flush_stats")
         return {f: getattr(st, f) for f, _ in st._fields_}
 
+    def set_plan_cache(self, entries: int) -> None:
+        check(self._lib.mlb_state_set_plan_cache(self._h, entries), "mlb_state_set_plan_cache")
+
     def set_timing(self, enable: bool = True) -> None:
         check(self._lib.mlb_state_set_timing(self._h, 1 if enable else 0), "mlb_state_set_timing")
 

@@ -407,3 +407,32 @@ def test_reference_core_routes_to_engine(gpu):
                                  shape=(2 << n,)).view(np.complex128)
     assert np.abs(host - want).max() < TOL
     core.quantum_state_destroy(qs)
+
+
+def test_plan_cache_replays_repeated_shapes(gpu):
+    """A repeated circuit shape (same gates and qubits, new angles) reuses the
+    cached plan and replays its launches as a graph; amplitudes are
+    bit-identical to an uncached state's.  A new shape misses; the least
+    recently used plan is evicted at capacity."""
+    n = 16
+    shapes = [brickwork(n, 8, s, zz_every=3) for s in (1, 2, 3)]  # same shape, new angles
+    other = brickwork(n, 5, 9)  # different depth: a new shape
+    with StateVector(n) as cached, StateVector(n) as plain:
+        cached.set_plan_cache(2)
+        hits = []
+        for g in shapes + [other, shapes[0]]:
+            for sv in (cached, plain):
+                sv.reset()
+                sv.run(g)
+                sv.flush()
+            hits.append(cached.flush_stats()["plan_cache_hit"])
+            assert np.array_equal(cached.amplitudes(), plain.amplitudes())
+        assert hits == [0, 1, 1, 0, 1]
+        cached.set_plan_cache(1)  # shrinking drops the cache
+        cached.reset()
+        cached.run(other)
+        cached.flush()
+        assert cached.flush_stats()["plan_cache_hit"] == 0
+        a = cached.amplitudes()
+        want = B.port_run(n, other)
+        assert np.abs(a - want).max() < TOL
