@@ -29,8 +29,8 @@ namespace mlb {
 namespace {
 
 template <typename Real> struct TileCfg;
-template <> struct TileCfg<double> {  // complex128: 2^12 amps = 64 KiB per CTA
-  static constexpr int TB = 12, RB = 3, NT = 256, MINB = 2, SW_SHIFT = 3, SW_MASK = 7, GPT = 1;
+template <> struct TileCfg<double> {  // complex128: 2^13 amps = 128 KiB per CTA (one CTA per SM)
+  static constexpr int TB = 13, RB = 4, NT = 256, MINB = 1, SW_SHIFT = 3, SW_MASK = 7, GPT = 1;
 };
 template <> struct TileCfg<float> {   // complex64: 2^13 amps = 64 KiB per CTA
   static constexpr int TB = 13, RB = 4, NT = 256, MINB = 2, SW_SHIFT = 4, SW_MASK = 15, GPT = 1;

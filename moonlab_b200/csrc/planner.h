@@ -19,7 +19,7 @@ inline int popc(uint64_t x) { return __builtin_popcountll(x); }
 struct Geo {
   int TB, RB;
 };
-inline Geo geo(int dtype) { return dtype == MLB_C128 ? Geo{12, 3} : Geo{13, 4}; }
+inline Geo geo(int dtype) { return dtype == MLB_C128 ? Geo{13, 4} : Geo{13, 4}; }  // same tile shape for both dtypes
 
 // Non-diagonal target qubits of an op (must lie inside a tile) and all the
 // qubits it touches (targets, controls, diagonal keys).
