@@ -162,41 +162,26 @@ def reference_sample(n: int, budget_s: float, gates):
 
 
 # ---------------------------------------------------------------------------
-# distributed plumbing
+# replicas over several GPUs (moonlab_b200.replicas)
 # ---------------------------------------------------------------------------
 def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    return ws, rank, local
+    from moonlab_b200 import replicas
+    return replicas.init()
 
 
 def dist_max(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from moonlab_b200 import replicas
+    return replicas.max_over_ranks(x, ws)
 
 
 def dist_barrier(ws: int):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from moonlab_b200 import replicas
+    replicas.barrier(ws)
 
 
 def dist_done(ws: int):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from moonlab_b200 import replicas
+    replicas.done(ws)
 
 
 # ---------------------------------------------------------------------------
@@ -227,6 +212,7 @@ def run_reference(args, ws, rank):
 
 def run_b200(args, ws, rank, local):
     import torch
+    from moonlab_b200 import replicas
     from moonlab_b200 import StateVector, _lib, kernel_launches
     from moonlab_b200.circuits import config_c2
 
@@ -348,7 +334,8 @@ def run_b200(args, ws, rank, local):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": ws / t_max, "unit": "circuits/s", "n_gpus": ws,
+            "metric": METRIC, "value": replicas.job_throughput(1.0, ws, t_max), "unit": "circuits/s",
+            "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic seeded circuit (splitmix64 0xC2)",
@@ -362,7 +349,8 @@ def run_b200(args, ws, rank, local):
                          "algorithmic_bytes_per_pass": per_pass_bytes},
             "c64": c64,
             "fused_c64": fused,
-            "e2e": {"value": ws / e2e_s, "unit": "circuits/s", "h2d_bytes_per_step": int(h2d),
+            "e2e": {"value": replicas.job_throughput(1.0, ws, e2e_s), "unit": "circuits/s",
+                    "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
