@@ -319,9 +319,10 @@ def run_b200(args, ws, rank, local):
     fused["kernel"] = "k_fused"
 
     sv.close()
-    serving = None if args.no_serving else serving_leg(args, local)
+    serving = None if args.no_serving else serving_leg(args, local,
+                                                       rank == 0 and ws == 1 and not args.no_cpu_baseline)
     sweep = None if args.no_sweep else gate_sweep_leg(local, peak)
-    vqe = None if args.no_vqe else vqe_leg(local)
+    vqe = None if args.no_vqe else vqe_leg(local, rank == 0 and ws == 1 and not args.no_cpu_baseline)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -365,21 +366,57 @@ def run_b200(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def serving_leg(args, local):
+def serving_leg(args, local, with_cpu: bool):
     """The request stream (Poisson arrivals; qubits U{10..28}, depth
     U{10..100}, shots U{1..4096}, dtype 50/50) on this rank's GPU through
     the continuous-batching server: first all requests at once (capacity,
-    circuits/s), then paced at --serve-rate (latency p50/p99 at that load).
-    Latency = submit to result on the host clock; circuits/s = requests /
-    (last result - first submit)."""
+    circuits/s), then paced at --serve-rate (latency p50/p99 at that load),
+    then 100 requests at each rate of a sweep, reporting the highest rate
+    whose p99 meets the stated target.  Latency = submit to result on the
+    host clock; circuits/s = requests / (last result - first submit).  With
+    with_cpu, the reference's moonlab_qgtl_execute is timed on the host on
+    up to 12 requests of <= 16 qubits beside the engine's time for the same
+    requests run one at a time."""
     from moonlab_b200.circuits import config_c5
     from moonlab_b200.serving import Server, request_circuit, run_load
     reqs = config_c5(num=args.serve_requests, rate=args.serve_rate)
     circ = [request_circuit(r) for r in reqs]
     workers = 8
+    p99_target_ms = 2000.0
+    sweep = []
     with Server(device=local, workers=workers) as srv:
         sat = run_load(srv, reqs, time_scale=0.0, circuits=circ)
         paced = run_load(srv, reqs, time_scale=1.0, circuits=circ)
+        # arrival-rate sweep: 100 requests of the stream re-timed at each rate
+        for lam in (8.0, 12.0, 16.0, 20.0):
+            sub = config_c5(num=100, rate=lam, seed=0xC5)
+            sr = run_load(srv, sub, time_scale=1.0)
+            sweep.append({"rate_per_s": lam, "circuits_per_s": sr["circuits_per_s"], "p50_ms": sr["p50_s"] * 1e3,
+                          "p99_ms": sr["p99_s"] * 1e3})
+        # per-request service time of small requests alone (for the CPU comparison)
+        small = [i for i, r in enumerate(reqs) if r.n <= 16][:12]
+        gpu_alone = []
+        for i in small:
+            r = reqs[i]
+            _, info = srv.wait(srv.submit(r.n, circ[i], r.shots, r.seed, "c64" if r.dtype else "c128"))
+            gpu_alone.append(info["done_s"] - info["submit_s"])
+    meets = [x["rate_per_s"] for x in sweep if x["p99_ms"] <= p99_target_ms]
+    cpu = None
+    if with_cpu:
+        try:  # the reference's moonlab_qgtl_execute on the same small requests (all host threads)
+            from oracle import bindings as B
+            t_cpu = []
+            for i in small:
+                r = reqs[i]
+                t0 = time.perf_counter()
+                B.ref_qgtl_execute(r.n, circ[i], r.shots, r.seed, want_probs=False)
+                t_cpu.append(time.perf_counter() - t0)
+            cpu = {"kind": "reference", "cores": os.cpu_count(),
+                   "sample": f"{len(small)} requests with <= 16 qubits through moonlab_qgtl_execute",
+                   "mean_service_ms": 1e3 * sum(t_cpu) / len(t_cpu),
+                   "b200_mean_service_ms": 1e3 * sum(gpu_alone) / len(gpu_alone)}
+        except Exception as e:  # reported, never replaced
+            cpu = {"kind": "reference", "sample": f"unavailable: {e}"}
     return {
         "workload": (f"{len(reqs)} requests of the Poisson stream (seed 0xC5): qubits U{{10..28}}, "
                      "depth U{10..100} brickwork, shots U{1..4096}, c128/c64 50/50"),
@@ -389,6 +426,10 @@ def serving_leg(args, local):
         "saturated_circuits_per_s": sat["circuits_per_s"], "saturated_p99_ms": sat["p99_s"] * 1e3,
         "peak_running": paced["stats"]["peak_running"],
         "peak_reserved_gib": paced["stats"]["peak_reserved_bytes"] / 2**30,
+        "p99_target_ms": p99_target_ms, "rate_sweep": sweep,
+        "max_rate_meeting_p99_per_s": max(meets) if meets else None,
+        "small_batches": paced["stats"]["small_batches"], "plan_cache_hits": paced["stats"]["plan_cache_hits"],
+        "cpu_reference": cpu,
     }
 
 
@@ -438,7 +479,7 @@ def gate_sweep_leg(local, peak):
     return out
 
 
-def vqe_leg(local):
+def vqe_leg(local, with_cpu: bool):
     """VQE adjoint gradient: hardware-efficient ansatz N = 20, L = 8 (320
     parameters), 80 random 2-local Pauli terms, a batch of 256 parameter
     vectors in one call, complex128 and complex64; host parameters in,
@@ -459,6 +500,27 @@ def vqe_leg(local):
         p.close()
     res["c64_max_rel_grad_err"] = float(np.abs(grads["c64"] - grads["c128"]).max() /
                                         max(1e-300, np.abs(grads["c128"]).max()))
+    if with_cpu:  # the reference's moonlab_vqe_gradient at N = 12 (minutes per vector at N = 20)
+        try:
+            from oracle import bindings as B
+            small = config_c4(n=12, layers=8, batch=64, seed=0xC4)
+            p12 = HEAProblem(12, 8, small.coeffs, xmasks=small.xmasks, zmasks=small.zmasks, device=local)
+            p12.evaluate(small.params[:4])
+            t0 = time.perf_counter()
+            p12.evaluate(small.params)
+            gpu12 = len(small.params) / (time.perf_counter() - t0)
+            p12.close()
+            solver = B.RefSolver(12, 8, small.paulis, small.coeffs)
+            t0 = time.perf_counter()
+            for k in range(2):
+                solver.gradient(small.params[k])
+            cpu12 = 2 / (time.perf_counter() - t0)
+            solver.close()
+            res["cpu_reference"] = {"kind": "reference", "cores": os.cpu_count(),
+                                    "sample": "moonlab_vqe_gradient, N=12 L=8, 48 terms, 2 vectors",
+                                    "vectors_per_s": cpu12, "b200_c128_vectors_per_s_same_problem": gpu12}
+        except Exception as e:  # reported, never replaced
+            res["cpu_reference"] = {"kind": "reference", "sample": f"unavailable: {e}"}
     return res
 
 
