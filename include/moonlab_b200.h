@@ -57,7 +57,9 @@ typedef enum { MLB_C128 = 0, MLB_C64 = 1 } mlb_dtype_t;
 typedef enum {
     MLB_EXEC_TILED = 0,  /* default: gates grouped into shared-memory tile passes */
     MLB_EXEC_EAGER = 1,  /* one full-state kernel per gate (the per-gate path) */
-    MLB_EXEC_FUSED = 2   /* complex64 states: gates fused into dense k<=5-qubit blocks */
+    MLB_EXEC_FUSED = 2   /* complex64 states: gates fused into dense k<=5-qubit blocks on the
+                            tensor cores; states under 13 qubits and ops on more than 5 qubits
+                            run as tile passes */
 } mlb_exec_mode_t;
 
 /* Gate operation kinds understood by the engine (mlb_op_t.kind). */

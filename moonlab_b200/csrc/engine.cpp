@@ -421,7 +421,7 @@ std::vector<uint64_t> plan_shape(const mlb_state* s, const std::vector<mlb_op_t>
 }
 
 // Fused complex64 path: dense <= 5-qubit blocks on the tensor cores.
-int flush_fused(mlb_state* s, const std::vector<mlb_op_t>& ops) {
+int flush_fused(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_t& st) {
   fused::Plan P;
   int rc = fused::plan(ops, s->n, P);
   if (rc) return fail(rc, "fused path: an op spans more than 5 qubits or the state has < 13 qubits");
@@ -441,8 +441,6 @@ int flush_fused(mlb_state* s, const std::vector<mlb_op_t>& ops) {
   const FusedBlockDev* d_blocks = reinterpret_cast<const FusedBlockDev*>(s->d_plan);
   const uint8_t* d_images = reinterpret_cast<const uint8_t*>(s->d_plan) + ioff;
   cudaMemsetAsync(s->d_ferr, 0, sizeof(int), s->stream);
-  mlb_flush_stats_t st{};
-  if (s->timing) cudaEventRecord(s->t0, s->stream);
   for (const auto& dp : P.dev_passes) {
     rc = launch_fused_pass(s->amp, (int)s->n, dp, d_blocks, d_images, s->d_ferr, s->num_sms, s->stream);
     if (rc) return fail(rc, "fused pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -450,49 +448,19 @@ int flush_fused(mlb_state* s, const std::vector<mlb_op_t>& ops) {
     st.kernel_launches++;
     st.bytes_moved += 2 * 8 * (1ull << s->n);
   }
-  if (s->timing) {
-    cudaEventRecord(s->t1, s->stream);
-    s->timed_pending = true;
-  }
   cudaMemcpyAsync(s->h_ferr, s->d_ferr, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
   s->ferr_pending = true;
-  st.ops = ops.size();
-  st.dense_blocks = P.dev_blocks.size();
-  st.segments = P.dev_blocks.size();
-  s->stats = st;
+  st.ops += ops.size();
+  st.dense_blocks += P.dev_blocks.size();
+  st.segments += P.dev_blocks.size();
   return MLB_OK;
 }
 
-int flush_impl(mlb_state* s) {
-  if (s->queue.empty()) return MLB_OK;
-  DeviceGuard dg(s->device);
-  mlb_flush_stats_t st{};
+// Tile passes for ops (tiled mode, and the parts of a fused flush that need
+// them), the plan taken from the state's plan cache when the shape repeats.
+int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_t& st) {
   const uint64_t dim = 1ull << s->n;
   const uint64_t ab = s->dtype == MLB_C128 ? 16 : 8;
-  if (s->mode == MLB_EXEC_EAGER) {
-    if (s->timing) cudaEventRecord(s->t0, s->stream);
-    for (const auto& o : s->queue) {
-      int rc = launch_gate(s->dtype, s->amp, (int)s->n, o, s->stream);
-      if (rc) { s->queue.clear(); return fail(rc, "gate launch failed: %s", cudaGetErrorString(cudaGetLastError())); }
-      st.ops++;
-      st.passes++;
-      st.kernel_launches++;
-      const int c = popc(o.cmask);
-      uint64_t touched = dim >> c;
-      if (o.kind == MLB_OP_PHASE) touched = dim >> popc(o.cmask);
-      st.bytes_moved += 2 * ab * touched;
-    }
-    s->queue.clear();
-    if (s->timing) {
-      cudaEventRecord(s->t1, s->stream);
-      s->timed_pending = true;
-    }
-    s->stats = st;
-    return MLB_OK;
-  }
-  std::vector<mlb_op_t> ops = s->fuse1q ? fuse_1q_runs(s->queue, s->n) : s->queue;
-  s->queue.clear();
-  if (s->mode == MLB_EXEC_FUSED) return flush_fused(s, ops);
   // the plan: from the cache when this shape ran before, else planned now
   mlb_state::PlanEntry local;
   mlb_state::PlanEntry* E = &local;
@@ -551,7 +519,6 @@ int flush_impl(mlb_state* s) {
     }
     return MLB_OK;
   };
-  if (s->timing) cudaEventRecord(s->t0, s->stream);
   if (s->plan_cache_cap && E != &local) {
     // replay the captured launches (capture once per plan buffer)
     if (E->exec && E->graph_dplan != s->d_plan) {
@@ -583,12 +550,62 @@ int flush_impl(mlb_state* s) {
   } else if ((rc = launch_passes())) {
     return fail(rc, "tile pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
-  st.passes = E->passes.size();
-  st.kernel_launches = E->passes.size();
-  st.bytes_moved = E->passes.size() * 2 * ab * dim;
-  st.ops = ops.size();
-  st.segments = E->segs.size();
+  st.passes += E->passes.size();
+  st.kernel_launches += E->passes.size();
+  st.bytes_moved += E->passes.size() * 2 * ab * dim;
+  st.ops += ops.size();
+  st.segments += E->segs.size();
   st.plan_cache_hit = hit ? 1 : 0;
+  return MLB_OK;
+}
+
+int flush_impl(mlb_state* s) {
+  if (s->queue.empty()) return MLB_OK;
+  DeviceGuard dg(s->device);
+  mlb_flush_stats_t st{};
+  const uint64_t dim = 1ull << s->n;
+  const uint64_t ab = s->dtype == MLB_C128 ? 16 : 8;
+  if (s->mode == MLB_EXEC_EAGER) {
+    if (s->timing) cudaEventRecord(s->t0, s->stream);
+    for (const auto& o : s->queue) {
+      int rc = launch_gate(s->dtype, s->amp, (int)s->n, o, s->stream);
+      if (rc) { s->queue.clear(); return fail(rc, "gate launch failed: %s", cudaGetErrorString(cudaGetLastError())); }
+      st.ops++;
+      st.passes++;
+      st.kernel_launches++;
+      const int c = popc(o.cmask);
+      uint64_t touched = dim >> c;
+      if (o.kind == MLB_OP_PHASE) touched = dim >> popc(o.cmask);
+      st.bytes_moved += 2 * ab * touched;
+    }
+    s->queue.clear();
+    if (s->timing) {
+      cudaEventRecord(s->t1, s->stream);
+      s->timed_pending = true;
+    }
+    s->stats = st;
+    return MLB_OK;
+  }
+  std::vector<mlb_op_t> ops = s->fuse1q ? fuse_1q_runs(s->queue, s->n) : s->queue;
+  s->queue.clear();
+  if (s->timing) cudaEventRecord(s->t0, s->stream);
+  int rc = MLB_OK;
+  if (s->mode != MLB_EXEC_FUSED || s->n < (uint32_t)fused::kTileBits) {
+    rc = flush_tiled(s, ops, st);
+  } else {
+    // fused blocks for runs of ops on <= 5 qubits; a wider op (a many-
+    // controlled gate) runs as a tile pass between them, in order
+    size_t i = 0;
+    while (!rc && i < ops.size()) {
+      size_t j = i;
+      const bool wide = popc(op_qubits(ops[i])) > fused::kBlockQubits;
+      while (j < ops.size() && (popc(op_qubits(ops[j])) > fused::kBlockQubits) == wide) j++;
+      const std::vector<mlb_op_t> run(ops.begin() + i, ops.begin() + j);
+      rc = wide ? flush_tiled(s, run, st) : flush_fused(s, run, st);
+      i = j;
+    }
+  }
+  if (rc) return rc;
   if (s->timing) {
     cudaEventRecord(s->t1, s->stream);
     s->timed_pending = true;
@@ -777,8 +794,8 @@ int mlb_state_set_exec_mode(mlb_state_t* s, int mode) {
   if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
   if (mode != MLB_EXEC_TILED && mode != MLB_EXEC_EAGER && mode != MLB_EXEC_FUSED)
     return fail(MLB_ERR_NOT_SUPPORTED, "exec mode %d not available", mode);
-  if (mode == MLB_EXEC_FUSED && (s->dtype != MLB_C64 || s->n < 13))
-    return fail(MLB_ERR_NOT_SUPPORTED, "the fused path needs a complex64 state of >= 13 qubits");
+  if (mode == MLB_EXEC_FUSED && s->dtype != MLB_C64)
+    return fail(MLB_ERR_NOT_SUPPORTED, "the fused path runs on complex64 states");
   int rc = flush_impl(s);
   if (rc) return rc;
   s->mode = mode;

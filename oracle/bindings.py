@@ -112,6 +112,16 @@ def port_run(n: int, gates) -> np.ndarray:
     return a
 
 
+def port_run_from(n: int, gates, state) -> np.ndarray:
+    """Gate records applied to a given state (copy) by the restatement."""
+    a = np.array(state, dtype=np.complex128, copy=True)
+    g = to_svo(gates)
+    rc = port().svo_apply_circuit(_dp(a.view(np.float64)), n, g, len(g))
+    if rc:
+        raise RuntimeError(f"svo_apply_circuit failed: {rc}")
+    return a
+
+
 def port_probabilities(a: np.ndarray, rule: int = 0) -> np.ndarray:
     lib = port()
     n = int(a.size).bit_length() - 1

@@ -51,9 +51,32 @@ def test_fused_fidelity_vs_oracle(gpu, n, depth):
     assert err < 1e-3
 
 
-def test_fused_mode_needs_complex64_and_13_qubits(gpu):
+def test_fused_mode_falls_back_to_tile_passes(gpu):
+    """complex128 states refuse the fused mode; a complex64 state under 13
+    qubits, and an op on more than 5 qubits inside a fused circuit, run as
+    tile passes in order with the fused blocks."""
     from moonlab_b200._lib import MlbError
     with StateVector(14, "c128") as sv, pytest.raises(MlbError):
         sv.set_exec_mode("fused")
-    with StateVector(12, "c64") as sv, pytest.raises(MlbError):
+    g12 = brickwork(12, 6, 3)
+    got, st = run_fused(12, g12)
+    assert st["dense_blocks"] == 0
+    assert np.abs(got - B.port_run(12, g12)).max() < 1e-5
+    n = 16
+    with StateVector(n, "c64") as sv:
         sv.set_exec_mode("fused")
+        g = brickwork(n, 4, 8)
+        sv.run(g[: len(g) // 2])
+        sv.mcx([0, 3, 7, 9, 12], 15)  # 6 qubits: a tile pass between fused runs
+        sv.run(g[len(g) // 2:])
+        got = sv.amplitudes().astype(np.complex128)
+        st = sv.flush_stats()
+    a = B.port_run(n, g[: len(g) // 2])
+    idx = np.arange(1 << n)
+    ctrl = (1 << 0) | (1 << 3) | (1 << 7) | (1 << 9) | (1 << 12)
+    sel = (idx & ctrl) == ctrl
+    b = a.copy()
+    b[sel] = a[idx[sel] ^ (1 << 15)]
+    want = B.port_run_from(n, g[len(g) // 2:], b)
+    assert st["dense_blocks"] > 0
+    assert np.abs(got - want).max() < 1e-5
