@@ -16,9 +16,11 @@
 // 128-lane x 64-column FP32 accumulator in tensor memory.
 //
 // Per block: every thread (one per tile row m) converts its 32 amplitudes
-// from the FP32 tile into the bf16 operand rows (K-major, 128-byte swizzle),
-// the block's operand image (prepared on the host, 16 KiB) is copied in, one
-// thread issues the MMAs and commits them to an mbarrier, and after the
+// from the FP32 tile into its row of the bf16 amplitude operand and stores
+// it to tensor memory (tcgen05.st, row per lane, two bf16 per column: the
+// operand-A layout of an A-from-TMEM MMA); the block's U' image (prepared
+// on the host, 16 KiB, K-major 128-byte swizzle) comes into shared memory;
+// one thread issues the MMAs and commits them to an mbarrier, and after the
 // commit arrives every warp reads its 32 accumulator lanes back
 // (tcgen05.ld 32x32b, 64 columns) into the FP32 tile.
 //
@@ -44,8 +46,7 @@ namespace {
 constexpr int kFThreads = 256;
 constexpr int kTileAmps = 1 << 13;
 // shared-memory layout (bytes from a 1024-byte aligned base)
-constexpr uint32_t kAHi = 0;          // 256 rows x 128 B
-constexpr uint32_t kALo = 32768;
+// (0 .. 64 KiB: unused since the amplitude operand lives in tensor memory)
 constexpr uint32_t kBHi = 65536;      // 64 rows x 128 B, then lo
 constexpr uint32_t kBLo = 73728;
 constexpr uint32_t kTile0 = 81920;    // two tile buffers of 2^13 float2 (64 KiB each)
@@ -59,7 +60,8 @@ constexpr int kMaxBlocks = 64;        // blocks per pass (the planner splits lon
 constexpr uint32_t kHiDep = kRoff + kMaxBlocks * 64;  // 16 x uint64: global offsets of tile bits 9..12
 constexpr uint32_t kSmemUsed = kHiDep + 16 * 8;
 constexpr uint32_t kSmemBytes = kSmemUsed + 1024;  // alignment slack
-constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kTmemCols = 256;  // D: columns 0..127 (64 per half); A: 128..255
+constexpr uint32_t kACol = 128;      // A of half h: hi at kACol + 64 h, lo at kACol + 64 h + 32
 constexpr long long kWaitLimit = 1ll << 22;      // try_wait rounds before giving up
 
 // instruction descriptor: D = F32, A = B = BF16, both K-major, N = 64, M = 128
@@ -89,6 +91,31 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t 
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
       "}\n" ::"r"(tmem_d),
       "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// A from tensor memory (row per lane, K packed two bf16 per column), B from
+// shared memory.
+__device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t"
+      "}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// 32 consecutive columns of this thread's lane.
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+      "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]),
+      "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]),
+      "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+      : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
@@ -288,12 +315,11 @@ __global__ void __launch_bounds__(kFThreads, 1)
             }
           }
         }
-        uint8_t* ahi = sm + kAHi + m * 128;
-        uint8_t* alo = sm + kALo + m * 128;
-        const uint32_t sx = m & 7u;
+        // row m's operand words: word j holds K elements 2j, 2j+1 (re of r for
+        // K < 32, im of r - 32 above), hi and lo parts
+        uint32_t whi[32], wlo[32];
 #pragma unroll
-        for (int c = 0; c < 4; c++) {  // chunk c: r = 8c .. 8c+7
-          uint32_t rh[4], rl[4], ih[4], il[4];
+        for (int c = 0; c < 4; c++) {
 #pragma unroll
           for (int w = 0; w < 4; w++) {
             const float2 a0 = tile[ebase ^ roff[8 * c + 2 * w]];
@@ -301,17 +327,20 @@ __global__ void __launch_bounds__(kFThreads, 1)
             const __nv_bfloat162 hre = __floats2bfloat162_rn(a0.x, a1.x);
             const __nv_bfloat162 him = __floats2bfloat162_rn(a0.y, a1.y);
             const float2 fre = __bfloat1622float2(hre), fim = __bfloat1622float2(him);
-            rh[w] = *reinterpret_cast<const uint32_t*>(&hre);
-            ih[w] = *reinterpret_cast<const uint32_t*>(&him);
-            rl[w] = pack_bf16x2(a0.x - fre.x, a1.x - fre.y);
-            il[w] = pack_bf16x2(a0.y - fim.x, a1.y - fim.y);
+            whi[4 * c + w] = *reinterpret_cast<const uint32_t*>(&hre);
+            whi[16 + 4 * c + w] = *reinterpret_cast<const uint32_t*>(&him);
+            wlo[4 * c + w] = pack_bf16x2(a0.x - fre.x, a1.x - fre.y);
+            wlo[16 + 4 * c + w] = pack_bf16x2(a0.y - fim.x, a1.y - fim.y);
           }
-          *reinterpret_cast<uint4*>(ahi + (((uint32_t)c ^ sx) << 4)) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-          *reinterpret_cast<uint4*>(ahi + (((uint32_t)(c + 4) ^ sx) << 4)) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-          *reinterpret_cast<uint4*>(alo + (((uint32_t)c ^ sx) << 4)) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-          *reinterpret_cast<uint4*>(alo + (((uint32_t)(c + 4) ^ sx) << 4)) = make_uint4(il[0], il[1], il[2], il[3]);
         }
+        // this warp's lane quadrant: row m = 128 h + 32 qd + lane
+        const uint32_t h = m >> 7, qd = (m >> 5) & 3u;
+        const uint32_t ta = tmem + ((qd * 32u) << 16) + kACol + h * 64u;
+        tmem_st32(ta, whi);
+        tmem_st32(ta + 32u, wlo);
+        asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
       }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       __syncthreads();
 
@@ -322,12 +351,12 @@ __global__ void __launch_bounds__(kFThreads, 1)
           for (int h = 0; h < 2; h++) {
 #pragma unroll
             for (int kc = 0; kc < 3; kc++) {
-              const uint32_t a0 = sbase + (kc == 1 ? kALo : kAHi) + (uint32_t)h * 16384u;
+              const uint32_t a0 = tmem + kACol + (uint32_t)h * 64u + (kc == 1 ? 32u : 0u);
               const uint32_t b0 = sbase + (kc == 2 ? kBLo : kBHi);
 #pragma unroll
               for (int kk = 0; kk < 4; kk++)
-                mma_bf16(tmem + (uint32_t)h * 64u, sdesc(a0 + kk * 32), sdesc(b0 + kk * 32),
-                         (kc | kk) != 0 ? 1u : 0u);
+                mma_bf16_ts(tmem + (uint32_t)h * 64u, a0 + kk * 8u, sdesc(b0 + kk * 32),
+                            (kc | kk) != 0 ? 1u : 0u);
             }
             // half h done -> its mbarrier (commit covers all earlier MMAs of this thread)
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
