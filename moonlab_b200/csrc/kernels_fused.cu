@@ -24,11 +24,13 @@
 // commit arrives every warp reads its 32 accumulator lanes back
 // (tcgen05.ld 32x32b, 64 columns) into the FP32 tile.
 //
-// Pipelining: the tile is double-buffered; while the tensor cores work on
-// tile t, 16-byte async copies (cp.async) bring tile t + grid into the other
-// buffer, so the HBM read overlaps the block math.  Each block's operand
-// image comes by one bulk copy completing on its own mbarrier, overlapping
-// the conversion of the amplitude operand.
+// Occupancy: a CTA of 4 warps (each warp owns one tensor-memory lane quadrant
+// and handles one row of each 128-row half) holds one tile buffer, the
+// block's operand image and 256 TMEM columns, so two CTAs share an SM: one
+// CTA's MMA waits and tile loads (16-byte async copies, cp.async) overlap
+// the other's operand conversion and readback.  Each block's operand image
+// comes by one bulk copy completing on its own mbarrier, requested as soon
+// as the previous block's MMAs have completed.
 //
 // Waits are bounded: if one runs out the kernel sets *err, waits once more
 // (bounded) for what it issued, frees its tensor memory and returns.
@@ -43,22 +45,22 @@ namespace mlb {
 
 namespace {
 
-constexpr int kFThreads = 256;
+constexpr int kFThreads = 128;       // 4 warps: each owns one TMEM lane quadrant (both halves)
 constexpr int kTileAmps = 1 << 13;
-// shared-memory layout (bytes from a 1024-byte aligned base)
-// (0 .. 64 KiB: unused since the amplitude operand lives in tensor memory)
-constexpr uint32_t kBHi = 65536;      // 64 rows x 128 B, then lo
-constexpr uint32_t kBLo = 73728;
-constexpr uint32_t kTile0 = 81920;    // two tile buffers of 2^13 float2 (64 KiB each)
+constexpr int kPairsPerThread = kTileAmps / 2 / kFThreads;  // 32
+// shared-memory layout (bytes from a 1024-byte aligned base); two CTAs per SM
+constexpr uint32_t kBHi = 0;          // 64 rows x 128 B, then lo
+constexpr uint32_t kBLo = 8192;
+constexpr uint32_t kTile0 = 16384;    // one tile buffer of 2^13 float2 (64 KiB)
 constexpr uint32_t kTileBytes = 65536;
-constexpr uint32_t kMbarMma = 212992;  // two: one per 128-row half
-constexpr uint32_t kMbarB = 213008;
-constexpr uint32_t kTmemSlot = 213016;
-constexpr uint32_t kFlag = 213020;
-constexpr uint32_t kRoff = 213024;    // per block: 32 swizzled column offsets (uint16), 16-byte aligned
+constexpr uint32_t kMbarMma = 81920;  // two: one per 128-row half
+constexpr uint32_t kMbarB = 81936;
+constexpr uint32_t kTmemSlot = 81944;
+constexpr uint32_t kFlag = 81948;
+constexpr uint32_t kRoff = 81952;     // per block: 32 swizzled column offsets (uint16), 16-byte aligned
 constexpr int kMaxBlocks = 64;        // blocks per pass (the planner splits longer passes)
-constexpr uint32_t kHiDep = kRoff + kMaxBlocks * 64;  // 16 x uint64: global offsets of tile bits 9..12
-constexpr uint32_t kSmemUsed = kHiDep + 16 * 8;
+constexpr uint32_t kHiDep = kRoff + kMaxBlocks * 64;  // 32 x uint64: global offsets of tile bits 8..12
+constexpr uint32_t kSmemUsed = kHiDep + kPairsPerThread * 8;
 constexpr uint32_t kSmemBytes = kSmemUsed + 1024;  // alignment slack
 constexpr uint32_t kTmemCols = 256;  // D: columns 0..127 (64 per half); A: 128..255
 constexpr uint32_t kACol = 128;      // A of half h: hi at kACol + 64 h, lo at kACol + 64 h + 32
@@ -81,16 +83,6 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
   d |= (uint64_t)1 << 46;               // descriptor version
   d |= (uint64_t)2 << 61;               // SWIZZLE_128B
   return d;
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t"
-      ".reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
-      "}\n" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
 // A from tensor memory (row per lane, K packed two bf16 per column), B from
@@ -216,7 +208,7 @@ __device__ __forceinline__ uint64_t tile_global(uint64_t gbase, uint32_t e, cons
   return g;
 }
 
-__global__ void __launch_bounds__(kFThreads, 1)
+__global__ void __launch_bounds__(kFThreads, 2)
     k_fused(float2* __restrict__ amp, FusedPassDev pass, const FusedBlockDev* __restrict__ blocks,
             const uint8_t* __restrict__ images, int* __restrict__ err) {
   extern __shared__ uint8_t smraw[];
@@ -253,7 +245,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
     for (int j = 0; j < 5; j++) o |= ((r >> j) & 1u) << blk.pos[j];
     roff_tab[i] = (uint16_t)tsw(o);
   }
-  if (tid < kTileAmps / 2 / kFThreads)
+  if (tid < kPairsPerThread)
     reinterpret_cast<uint64_t*>(sm + kHiDep)[tid] = tile_global(0, (uint32_t)tid * 2u * kFThreads, pass);
   __syncthreads();
 
@@ -268,38 +260,34 @@ __global__ void __launch_bounds__(kFThreads, 1)
   // a per-thread part (bits 0..8) and a per-i part (bits 9..12, shared table).
   const uint64_t my_off = tile_global(0, 2u * (uint32_t)tid, pass);
   const uint64_t* hidep = reinterpret_cast<const uint64_t*>(sm + kHiDep);
-  uint32_t my_sw[kTileAmps / 2 / kFThreads];
-#pragma unroll
-  for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) my_sw[i] = tsw((uint32_t)(i * kFThreads + tid) * 2u);
+  // tsw is linear over GF(2): tsw(256 i + 2 tid) = tsw(256 i) ^ tsw(2 tid), the
+  // first term a compile-time constant in the unrolled loops
+  const uint32_t my_sw0 = tsw(2u * (uint32_t)tid);
 
-  // prefetch of a tile into buffer `buf`: 16 async 16-byte copies per thread
-  auto prefetch = [&](uint64_t t, int buf) {
+  auto load_tile = [&](uint64_t t) {
     const uint64_t gb = tile_base(t, tmask) | my_off;
-    const uint32_t dst0 = sbase + kTile0 + (uint32_t)buf * kTileBytes;
-#pragma unroll
-    for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) cp_async16(dst0 + my_sw[i] * 8u, amp + (gb | hidep[i]));
+    const uint32_t dst0 = sbase + kTile0;
+#pragma unroll 8
+    for (int i = 0; i < kPairsPerThread; i++) cp_async16(dst0 + (my_sw0 ^ tsw((uint32_t)i * 2u * kFThreads)) * 8u, amp + (gb | hidep[i]));
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
 
   uint32_t ph_mma = 0, ph_b = 0;
   bool bad = false;
-  int buf = 0;
-  if ((uint64_t)blockIdx.x < pass.num_tiles) prefetch(blockIdx.x, 0);
-  // operand image of the first block; each later one is requested as soon as
-  // the MMAs reading the previous one have completed
   if (tid == 0 && (uint64_t)blockIdx.x < pass.num_tiles)
     bulk_load(sbase + kBHi, images + (size_t)blocks[pass.block_begin].image * 16384, 16384, bar_b);
-  for (uint64_t t = blockIdx.x; t < pass.num_tiles && !bad; t += gridDim.x, buf ^= 1) {
+  float2* tile = reinterpret_cast<float2*>(sm + kTile0);
+  for (uint64_t t = blockIdx.x; t < pass.num_tiles && !bad; t += gridDim.x) {
+    load_tile(t);
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    if (t + gridDim.x < pass.num_tiles) prefetch(t + gridDim.x, buf ^ 1);
-    float2* tile = reinterpret_cast<float2*>(sm + kTile0 + (uint32_t)buf * kTileBytes);
 
     for (uint32_t b = 0; b < pass.num_blocks; b++) {
       const FusedBlockDev blk = blocks[pass.block_begin + b];
-      // amplitude operand: this thread's row m = tid
-      {
-        const uint32_t m = (uint32_t)tid;
+      // amplitude operand: this thread's rows m = tid and 128 + tid
+#pragma unroll 1
+      for (uint32_t hh = 0; hh < 2; hh++) {
+        const uint32_t m = 128u * hh + (uint32_t)tid;
         const uint32_t ebase = tsw(deposit8(m, blk.q));
         uint32_t roff[32];
         {
@@ -367,26 +355,28 @@ __global__ void __launch_bounds__(kFThreads, 1)
           atomicOr((int*)flag, 1);  // operand copy not seen; no MMA issued
         }
       }
-      // Each warp waits for the MMAs of its own half and reads its 32
-      // accumulator lanes back; half 0 overlaps the MMAs of half 1.  The
-      // lane that sees half 1 complete (all MMAs done, B free) requests the
-      // next operand image.
+      // Each warp owns lane quadrant qd: half 0 first, then half 1 (half 0's
+      // readback overlaps half 1's MMAs); the lane that sees half 1 complete
+      // requests the next operand image.
       {
-        const uint32_t h = (uint32_t)warp >> 2, qd = (uint32_t)warp & 3u;
+        const uint32_t qd = (uint32_t)warp;
         __syncwarp();
-        int ok = 0;
-        if (lane == 0 && !*flag) {
-          ok = mbar_wait_bounded(bar_mma + 8u * h, ph_mma) ? 1 : 0;
-          if (!ok) atomicOr((int*)flag, 2);
-          if (ok && h == 1 && qd == 0) {
-            const bool more = b + 1 < pass.num_blocks || t + gridDim.x < pass.num_tiles;
-            const uint32_t nb = b + 1 < pass.num_blocks ? b + 1 : 0;
-            if (more)
-              bulk_load(sbase + kBHi, images + (size_t)blocks[pass.block_begin + nb].image * 16384, 16384, bar_b);
+#pragma unroll 1
+        for (uint32_t h = 0; h < 2; h++) {
+          int ok = 0;
+          if (lane == 0 && !*flag) {
+            ok = mbar_wait_bounded(bar_mma + 8u * h, ph_mma) ? 1 : 0;
+            if (!ok) atomicOr((int*)flag, 2);
+            if (ok && h == 1 && qd == 0) {
+              const bool more = b + 1 < pass.num_blocks || t + gridDim.x < pass.num_tiles;
+              const uint32_t nb = b + 1 < pass.num_blocks ? b + 1 : 0;
+              if (more)
+                bulk_load(sbase + kBHi, images + (size_t)blocks[pass.block_begin + nb].image * 16384, 16384,
+                          bar_b);
+            }
           }
-        }
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (ok) {
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          if (!ok) break;
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
           float d[64];
           tmem_ld64(tmem + ((qd * 32u) << 16) + h * 64u, d);
@@ -420,12 +410,13 @@ __global__ void __launch_bounds__(kFThreads, 1)
     // store
     {
       const uint64_t gb = tile_base(t, tmask) | my_off;
-#pragma unroll
-      for (int i = 0; i < kTileAmps / 2 / kFThreads; i++) {
-        const float4 v = *reinterpret_cast<const float4*>(tile + my_sw[i]);
+#pragma unroll 8
+      for (int i = 0; i < kPairsPerThread; i++) {
+        const float4 v = *reinterpret_cast<const float4*>(tile + (my_sw0 ^ tsw((uint32_t)i * 2u * kFThreads)));
         __stcs(reinterpret_cast<float4*>(amp + (gb | hidep[i])), v);
       }
     }
+    __syncthreads();  // the tile buffer is free for the next load
   }
 
   // leave no async copy or MMA in flight
@@ -460,7 +451,7 @@ int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlo
     cudaFuncSetAttribute(k_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
     attr_set_mask.fetch_or(bit, std::memory_order_release);
   }
-  uint64_t grid = (uint64_t)num_sms;
+  uint64_t grid = (uint64_t)num_sms * 2;  // two CTAs per SM
   if (grid > pass.num_tiles) grid = pass.num_tiles;
   k_fused<<<(unsigned)grid, kFThreads, kSmemBytes, stream>>>(reinterpret_cast<float2*>(amp), pass, d_blocks,
                                                              d_images, d_err);
