@@ -20,17 +20,22 @@
 // it to tensor memory (tcgen05.st, row per lane, two bf16 per column: the
 // operand-A layout of an A-from-TMEM MMA); the block's U' image (prepared
 // on the host, 16 KiB, K-major 128-byte swizzle) comes into shared memory;
-// one thread issues the MMAs and commits them to an mbarrier, and after the
-// commit arrives every warp reads its 32 accumulator lanes back
-// (tcgen05.ld 32x32b, 64 columns) into the FP32 tile.
+// per 128-row half one thread issues that half's MMAs and commits them to
+// the half's mbarrier, and after the commit arrives the half's warps read
+// their 32 accumulator lanes back (tcgen05.ld 32x32b) into the FP32 tile.
 //
-// Occupancy: a CTA of 4 warps (each warp owns one tensor-memory lane quadrant
-// and handles one row of each 128-row half) holds one tile buffer, the
+// Occupancy: a CTA of 8 warps (warp w owns tensor-memory lane quadrant w & 3
+// of half w >> 2, one tile row per thread) holds one tile buffer, the
 // block's operand image and 256 TMEM columns, so two CTAs share an SM: one
 // CTA's MMA waits and tile loads (16-byte async copies, cp.async) overlap
-// the other's operand conversion and readback.  Each block's operand image
-// comes by one bulk copy completing on its own mbarrier, requested as soon
-// as the previous block's MMAs have completed.
+// the other's operand conversion and readback.  A half's MMAs start as soon
+// as its own four warps have stored their rows (a named barrier per half),
+// and the two halves are issued from different SM sub-partitions: one thread
+// issues an MMA only every ~70 cycles, so one issuer alone would leave the
+// tensor core half idle at N = 64.  MMA descriptors are precomputed (the
+// per-MMA part is a constant add).  Each block's operand image comes by one
+// bulk copy completing on its own mbarrier, requested as soon as both
+// halves' MMAs have completed.
 //
 // Waits are bounded: if one runs out the kernel sets *err, waits once more
 // (bounded) for what it issued, frees its tensor memory and returns.
@@ -45,9 +50,9 @@ namespace mlb {
 
 namespace {
 
-constexpr int kFThreads = 128;       // 4 warps: each owns one TMEM lane quadrant (both halves)
+constexpr int kFThreads = 256;       // 8 warps: warp w owns TMEM lane quadrant w & 3 of half w >> 2
 constexpr int kTileAmps = 1 << 13;
-constexpr int kPairsPerThread = kTileAmps / 2 / kFThreads;  // 32
+constexpr int kPairsPerThread = kTileAmps / 2 / kFThreads;  // 16
 // shared-memory layout (bytes from a 1024-byte aligned base); two CTAs per SM
 constexpr uint32_t kBHi = 0;          // 64 rows x 128 B, then lo
 constexpr uint32_t kBLo = 8192;
@@ -57,10 +62,12 @@ constexpr uint32_t kMbarMma = 81920;  // two: one per 128-row half
 constexpr uint32_t kMbarB = 81936;
 constexpr uint32_t kTmemSlot = 81944;
 constexpr uint32_t kFlag = 81948;
-constexpr uint32_t kRoff = 81952;     // per block: 32 swizzled column offsets (uint16), 16-byte aligned
 constexpr int kMaxBlocks = 64;        // blocks per pass (the planner splits longer passes)
-constexpr uint32_t kHiDep = kRoff + kMaxBlocks * 64;  // 32 x uint64: global offsets of tile bits 8..12
-constexpr uint32_t kSmemUsed = kHiDep + kPairsPerThread * 8;
+constexpr uint32_t kColTab = 81952;   // per block: 32 swizzled column offsets (uint32)
+constexpr uint32_t kRowTab = kColTab + kMaxBlocks * 128;  // per block: 2 x 16 swizzled row-nibble offsets (uint16)
+constexpr uint32_t kHiDep = kRowTab + kMaxBlocks * 64;    // 16 x uint64: global offsets of tile bits 9..12
+constexpr uint32_t kImgTab = kHiDep + kPairsPerThread * 8;  // per block: operand image index (uint32)
+constexpr uint32_t kSmemUsed = kImgTab + kMaxBlocks * 4;
 constexpr uint32_t kSmemBytes = kSmemUsed + 1024;  // alignment slack
 constexpr uint32_t kTmemCols = 256;  // D: columns 0..127 (64 per half); A: 128..255
 constexpr uint32_t kACol = 128;      // A of half h: hi at kACol + 64 h, lo at kACol + 64 h + 32
@@ -97,17 +104,22 @@ __device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, ui
       "r"(tmem_a), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
-// 32 consecutive columns of this thread's lane.
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+// 8 consecutive columns of this thread's lane.
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* v) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};\n" ::"r"(taddr), "r"(v[0]),
+               "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
+}
+
+// 16 consecutive columns of this thread's lane (completion: tcgen05.wait::ld).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t* r = reinterpret_cast<uint32_t*>(v);
   asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
-      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
-      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n" ::"r"(taddr),
-      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
-      "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]),
-      "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]),
-      "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
-      : "memory");
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
 }
 
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
@@ -149,36 +161,17 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
-  uint32_t* r = reinterpret_cast<uint32_t*>(v);
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
-      "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
-      "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-        "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
-        "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
-        "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]),
-        "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]),
-        "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]),
-        "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
-        "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-}
-
 // XOR swizzle of the FP32 tile on bits 1..4 (pairs of amplitudes stay
 // together, so 16-byte async copies land whole): spreads rows of any stride
 // over the banks.
 __device__ __forceinline__ uint32_t tsw(uint32_t e) { return e ^ ((((e >> 5) ^ (e >> 9)) & 15u) << 1); }
 
-__device__ __forceinline__ uint32_t deposit8(uint32_t v, const uint8_t (&pos)[8]) {
+// Bits 0..nb-1 of v placed at tile bits pos[0..nb-1].
+template <int NB>
+__device__ __forceinline__ uint32_t deposit(uint32_t v, const uint8_t* pos) {
   uint32_t r = 0;
 #pragma unroll
-  for (int i = 0; i < 8; i++) r |= ((v >> i) & 1u) << pos[i];
+  for (int i = 0; i < NB; i++) r |= ((v >> i) & 1u) << pos[i];
   return r;
 }
 
@@ -216,6 +209,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
   const uint32_t sbase = smem_u32(sm);
   volatile int* flag = reinterpret_cast<volatile int*>(sm + kFlag);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t half = (uint32_t)warp >> 2, qd = (uint32_t)warp & 3u;  // row m = tid = 128 half + 32 qd + lane
   const uint32_t bar_mma = sbase + kMbarMma, bar_b = sbase + kMbarB;  // bar_mma + 8 h: half h
 
   if (warp == 0) {
@@ -230,24 +224,26 @@ __global__ void __launch_bounds__(kFThreads, 2)
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     *flag = 0;
   }
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTmemSlot);
 
-  // Column offsets of every block of the pass, swizzled once: tsw is linear
-  // over GF(2), so tsw(row | col) = tsw(row) ^ tsw(col) for disjoint bits.
-  uint16_t* roff_tab = reinterpret_cast<uint16_t*>(sm + kRoff);
+  // Per-block tables, swizzled once (tsw is linear over GF(2), so the offset
+  // of tile row m and column r is rowtab(m & 15) ^ rowtab(16 + (m >> 4)) ^ coltab(r)):
+  //   coltab: the 32 block columns r (block bits pos[0..4]);
+  //   rowtab: the 16 values of each nibble of m (tile bits q[0..3], q[4..7]).
+  uint32_t* coltab = reinterpret_cast<uint32_t*>(sm + kColTab);
+  uint16_t* rowtab = reinterpret_cast<uint16_t*>(sm + kRowTab);
+  uint32_t* imgtab = reinterpret_cast<uint32_t*>(sm + kImgTab);
   for (uint32_t i = tid; i < pass.num_blocks * 32u; i += kFThreads) {
     const FusedBlockDev blk = blocks[pass.block_begin + i / 32u];
-    const uint32_t r = i & 31u;
-    uint32_t o = 0;
-#pragma unroll
-    for (int j = 0; j < 5; j++) o |= ((r >> j) & 1u) << blk.pos[j];
-    roff_tab[i] = (uint16_t)tsw(o);
+    const uint32_t j = i & 31u;
+    coltab[i] = tsw(deposit<5>(j, blk.pos));
+    rowtab[i] = (uint16_t)tsw(j < 16 ? deposit<4>(j, blk.q) : deposit<4>(j - 16u, blk.q + 4));
+    if (j == 0) imgtab[i / 32u] = blk.image;
   }
   if (tid < kPairsPerThread)
     reinterpret_cast<uint64_t*>(sm + kHiDep)[tid] = tile_global(0, (uint32_t)tid * 2u * kFThreads, pass);
   __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTmemSlot);
 
   uint64_t hmask = (1ull << pass.num_low) - 1ull;
 #pragma unroll
@@ -260,145 +256,133 @@ __global__ void __launch_bounds__(kFThreads, 2)
   // a per-thread part (bits 0..8) and a per-i part (bits 9..12, shared table).
   const uint64_t my_off = tile_global(0, 2u * (uint32_t)tid, pass);
   const uint64_t* hidep = reinterpret_cast<const uint64_t*>(sm + kHiDep);
-  // tsw is linear over GF(2): tsw(256 i + 2 tid) = tsw(256 i) ^ tsw(2 tid), the
-  // first term a compile-time constant in the unrolled loops
+  // tsw(512 i + 2 tid) = tsw(512 i) ^ tsw(2 tid), the first term a
+  // compile-time constant in the unrolled loops
   const uint32_t my_sw0 = tsw(2u * (uint32_t)tid);
-
-  auto load_tile = [&](uint64_t t) {
-    const uint64_t gb = tile_base(t, tmask) | my_off;
-    const uint32_t dst0 = sbase + kTile0;
-#pragma unroll 8
-    for (int i = 0; i < kPairsPerThread; i++) cp_async16(dst0 + (my_sw0 ^ tsw((uint32_t)i * 2u * kFThreads)) * 8u, amp + (gb | hidep[i]));
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-  };
+  // this thread's lane quadrant in tensor memory
+  const uint32_t tlane = tmem + ((qd * 32u) << 16);
+  // operand-image descriptor; the start-address field (bits 0..13, address >> 4)
+  // of the other K chunks and of the lo image is this plus a constant (the
+  // shared window is below 256 KiB, so the field does not carry)
+  const uint64_t desc_b = sdesc(sbase + kBHi);
 
   uint32_t ph_mma = 0, ph_b = 0;
   bool bad = false;
   if (tid == 0 && (uint64_t)blockIdx.x < pass.num_tiles)
-    bulk_load(sbase + kBHi, images + (size_t)blocks[pass.block_begin].image * 16384, 16384, bar_b);
+    bulk_load(sbase + kBHi, images + (size_t)imgtab[0] * 16384, 16384, bar_b);
   float2* tile = reinterpret_cast<float2*>(sm + kTile0);
   for (uint64_t t = blockIdx.x; t < pass.num_tiles && !bad; t += gridDim.x) {
-    load_tile(t);
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    {
+      const uint64_t gb = tile_base(t, tmask) | my_off;
+      const uint32_t dst0 = sbase + kTile0;
+#pragma unroll 8
+      for (int i = 0; i < kPairsPerThread; i++)
+        cp_async16(dst0 + (my_sw0 ^ tsw((uint32_t)i * 2u * kFThreads)) * 8u, amp + (gb | hidep[i]));
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
     __syncthreads();
 
     for (uint32_t b = 0; b < pass.num_blocks; b++) {
-      const FusedBlockDev blk = blocks[pass.block_begin + b];
-      // amplitude operand: this thread's rows m = tid and 128 + tid
-#pragma unroll 1
-      for (uint32_t hh = 0; hh < 2; hh++) {
-        const uint32_t m = 128u * hh + (uint32_t)tid;
-        const uint32_t ebase = tsw(deposit8(m, blk.q));
-        uint32_t roff[32];
-        {
-          const uint4* rt = reinterpret_cast<const uint4*>(roff_tab + b * 32u);
+      const uint32_t ebase = rowtab[b * 32u + (tid & 15)] ^ rowtab[b * 32u + 16u + ((uint32_t)tid >> 4)];
+      const uint4* ct = reinterpret_cast<const uint4*>(coltab + b * 32u);
+      // Amplitude operand, row m = tid, in two groups of 16 columns r: word j
+      // holds K elements 2j, 2j+1 (re of r for K < 32, im of r - 32 above),
+      // hi and lo parts; group g fills words 8g..8g+7 of each quarter.
+      {
+        const uint32_t ta = tlane + kACol + half * 64u;
 #pragma unroll
-          for (int v = 0; v < 4; v++) {
-            const uint4 x = rt[v];
-            const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
+        for (int g = 0; g < 2; g++) {
+          uint32_t hre[8], him[8], lre[8], lim[8];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-              roff[v * 8 + 2 * k] = w4[k] & 0xffffu;
-              roff[v * 8 + 2 * k + 1] = w4[k] >> 16;
-            }
+          for (int c = 0; c < 4; c++) {  // columns 16 g + 4 c .. + 3
+            const uint4 o = ct[4 * g + c];
+            const float2 a0 = tile[ebase ^ o.x], a1 = tile[ebase ^ o.y];
+            const float2 a2 = tile[ebase ^ o.z], a3 = tile[ebase ^ o.w];
+            const __nv_bfloat162 h0 = __floats2bfloat162_rn(a0.x, a1.x), h1 = __floats2bfloat162_rn(a0.y, a1.y);
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(a2.x, a3.x), h3 = __floats2bfloat162_rn(a2.y, a3.y);
+            const float2 f0 = __bfloat1622float2(h0), f1 = __bfloat1622float2(h1);
+            const float2 f2 = __bfloat1622float2(h2), f3 = __bfloat1622float2(h3);
+            hre[2 * c] = *reinterpret_cast<const uint32_t*>(&h0);
+            him[2 * c] = *reinterpret_cast<const uint32_t*>(&h1);
+            hre[2 * c + 1] = *reinterpret_cast<const uint32_t*>(&h2);
+            him[2 * c + 1] = *reinterpret_cast<const uint32_t*>(&h3);
+            lre[2 * c] = pack_bf16x2(a0.x - f0.x, a1.x - f0.y);
+            lim[2 * c] = pack_bf16x2(a0.y - f1.x, a1.y - f1.y);
+            lre[2 * c + 1] = pack_bf16x2(a2.x - f2.x, a3.x - f2.y);
+            lim[2 * c + 1] = pack_bf16x2(a2.y - f3.x, a3.y - f3.y);
           }
+          tmem_st8(ta + 8u * g, hre);
+          tmem_st8(ta + 16u + 8u * g, him);
+          tmem_st8(ta + 32u + 8u * g, lre);
+          tmem_st8(ta + 48u + 8u * g, lim);
         }
-        // row m's operand words: word j holds K elements 2j, 2j+1 (re of r for
-        // K < 32, im of r - 32 above), hi and lo parts
-        uint32_t whi[32], wlo[32];
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-#pragma unroll
-          for (int w = 0; w < 4; w++) {
-            const float2 a0 = tile[ebase ^ roff[8 * c + 2 * w]];
-            const float2 a1 = tile[ebase ^ roff[8 * c + 2 * w + 1]];
-            const __nv_bfloat162 hre = __floats2bfloat162_rn(a0.x, a1.x);
-            const __nv_bfloat162 him = __floats2bfloat162_rn(a0.y, a1.y);
-            const float2 fre = __bfloat1622float2(hre), fim = __bfloat1622float2(him);
-            whi[4 * c + w] = *reinterpret_cast<const uint32_t*>(&hre);
-            whi[16 + 4 * c + w] = *reinterpret_cast<const uint32_t*>(&him);
-            wlo[4 * c + w] = pack_bf16x2(a0.x - fre.x, a1.x - fre.y);
-            wlo[16 + 4 * c + w] = pack_bf16x2(a0.y - fim.x, a1.y - fim.y);
-          }
-        }
-        // this warp's lane quadrant: row m = 128 h + 32 qd + lane
-        const uint32_t h = m >> 7, qd = (m >> 5) & 3u;
-        const uint32_t ta = tmem + ((qd * 32u) << 16) + kACol + h * 64u;
-        tmem_st32(ta, whi);
-        tmem_st32(ta + 32u, wlo);
         asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       }
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      __syncthreads();
-
-      if (tid == 0) {
+      // Each half's MMAs start once its four warps have stored their rows
+      // (named barrier 1 + half) and are issued by one thread of that half,
+      // on different SM sub-partitions (warps 0 and 5), so the two halves'
+      // MMA streams overlap.
+      if (half == 0) asm volatile("bar.sync 1, 128;\n" ::: "memory");
+      else asm volatile("bar.sync 2, 128;\n" ::: "memory");
+      if (tid == 0 || tid == 160) {
         if (mbar_wait_bounded(bar_b, ph_b)) {  // operand image landed
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+          const uint32_t a_h = tmem + kACol + half * 64u, d_h = tmem + half * 64u;
 #pragma unroll
-          for (int h = 0; h < 2; h++) {
+          for (int kc = 0; kc < 3; kc++) {
 #pragma unroll
-            for (int kc = 0; kc < 3; kc++) {
-              const uint32_t a0 = tmem + kACol + (uint32_t)h * 64u + (kc == 1 ? 32u : 0u);
-              const uint32_t b0 = sbase + (kc == 2 ? kBLo : kBHi);
-#pragma unroll
-              for (int kk = 0; kk < 4; kk++)
-                mma_bf16_ts(tmem + (uint32_t)h * 64u, a0 + kk * 8u, sdesc(b0 + kk * 32),
-                            (kc | kk) != 0 ? 1u : 0u);
-            }
-            // half h done -> its mbarrier (commit covers all earlier MMAs of this thread)
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                             bar_mma + 8u * (uint32_t)h)
-                         : "memory");
+            for (int kk = 0; kk < 4; kk++)
+              mma_bf16_ts(d_h, a_h + (kc == 1 ? 32u : 0u) + kk * 8u,
+                          desc_b + (uint64_t)(((kc == 2 ? kBLo : kBHi) + kk * 32u) >> 4), (kc | kk) != 0 ? 1u : 0u);
           }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                           bar_mma + 8u * half)
+                       : "memory");
         } else {
-          atomicOr((int*)flag, 1);  // operand copy not seen; no MMA issued
+          atomicOr((int*)flag, 1);  // operand copy not seen; this half's MMAs not issued
         }
       }
-      // Each warp owns lane quadrant qd: half 0 first, then half 1 (half 0's
-      // readback overlaps half 1's MMAs); the lane that sees half 1 complete
-      // requests the next operand image.
+      // Readback of this warp's 32 accumulator lanes of its half; warp 5 also
+      // waits for half 0 and then requests the next operand image.
       {
-        const uint32_t qd = (uint32_t)warp;
+        int ok = 0;
         __syncwarp();
-#pragma unroll 1
-        for (uint32_t h = 0; h < 2; h++) {
-          int ok = 0;
-          if (lane == 0 && !*flag) {
-            ok = mbar_wait_bounded(bar_mma + 8u * h, ph_mma) ? 1 : 0;
-            if (!ok) atomicOr((int*)flag, 2);
-            if (ok && h == 1 && qd == 0) {
-              const bool more = b + 1 < pass.num_blocks || t + gridDim.x < pass.num_tiles;
-              const uint32_t nb = b + 1 < pass.num_blocks ? b + 1 : 0;
-              if (more)
-                bulk_load(sbase + kBHi, images + (size_t)blocks[pass.block_begin + nb].image * 16384, 16384,
-                          bar_b);
-            }
+        if (lane == 0 && !*flag) {
+          ok = mbar_wait_bounded(bar_mma + 8u * half, ph_mma) ? 1 : 0;
+          if (ok && warp == 5) ok = mbar_wait_bounded(bar_mma, ph_mma) ? 1 : 0;  // and half 0
+          if (!ok) atomicOr((int*)flag, 2);
+          if (ok && warp == 5) {
+            const bool more = b + 1 < pass.num_blocks || t + gridDim.x < pass.num_tiles;
+            const uint32_t nb = b + 1 < pass.num_blocks ? b + 1 : 0;
+            if (more) bulk_load(sbase + kBHi, images + (size_t)imgtab[nb] * 16384, 16384, bar_b);
           }
-          ok = __shfl_sync(0xffffffffu, ok, 0);
-          if (!ok) break;
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok) {
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-          float d[64];
-          tmem_ld64(tmem + ((qd * 32u) << 16) + h * 64u, d);
-          const uint32_t m = h * 128u + qd * 32u + (uint32_t)lane;
-          const uint32_t ebase = tsw(deposit8(m, blk.q));
-          const uint4* rt = reinterpret_cast<const uint4*>(roff_tab + b * 32u);
+          const uint32_t td = tlane + half * 64u;
 #pragma unroll
-          for (int v = 0; v < 4; v++) {
-            const uint4 x = rt[v];
-            const uint32_t w4[4] = {x.x, x.y, x.z, x.w};
+          for (int g = 0; g < 2; g++) {  // columns r = 16 g .. 16 g + 15
+            float dre[16], dim[16];
+            tmem_ld16(td + 16u * g, dre);
+            tmem_ld16(td + 32u + 16u * g, dim);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-              const int r = v * 8 + 2 * k;
-              tile[ebase ^ (w4[k] & 0xffffu)] = make_float2(d[r], d[32 + r]);
-              tile[ebase ^ (w4[k] >> 16)] = make_float2(d[r + 1], d[32 + r + 1]);
+            for (int c = 0; c < 4; c++) {
+              const uint4 o = ct[4 * g + c];
+              tile[ebase ^ o.x] = make_float2(dre[4 * c], dim[4 * c]);
+              tile[ebase ^ o.y] = make_float2(dre[4 * c + 1], dim[4 * c + 1]);
+              tile[ebase ^ o.z] = make_float2(dre[4 * c + 2], dim[4 * c + 2]);
+              tile[ebase ^ o.w] = make_float2(dre[4 * c + 3], dim[4 * c + 3]);
             }
           }
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      __syncthreads();
-      if (*flag) {
+      // every thread that sets the flag reads it back here, so all agree
+      if (__syncthreads_or(*flag != 0)) {
         bad = true;
         break;
       }
@@ -421,14 +405,13 @@ __global__ void __launch_bounds__(kFThreads, 2)
 
   // leave no async copy or MMA in flight
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  if (bad && tid == 0) {  // flag bit 1: operand copy pending; bit 2: MMAs pending
+  if (bad && tid == 0) {  // flag bit 1: an operand copy may be pending
     atomicExch(err, 1);
     const int f = *flag;
     if (f & 1) mbar_wait_bounded(bar_b, ph_b);
-    if (f & 2) {
-      mbar_wait_bounded(bar_mma, ph_mma);
-      mbar_wait_bounded(bar_mma + 8, ph_mma);
-    }
+    // either half's MMAs may be in flight (the halves have separate issuers)
+    mbar_wait_bounded(bar_mma, ph_mma);
+    mbar_wait_bounded(bar_mma + 8, ph_mma);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();

@@ -42,18 +42,23 @@ def deposit(v, bits):
     return out
 
 
+def tile_bits(p):
+    """Qubits in a pass's tile: its low qubits plus its chosen high ones."""
+    return p["num_low"] + len(p["hbits"])
+
+
 def replay(plan, n, state):
     st = state.astype(np.complex128).copy()
     imgs = plan["images"].reshape(-1, 16384)
-    e = np.arange(1 << 13, dtype=np.int64)
     for p in plan["passes"]:
-        hb, L = p["hbits"], p["num_low"]
+        hb, L, tb = p["hbits"], p["num_low"], tile_bits(p)
+        e = np.arange(1 << tb, dtype=np.int64)
         rest = [q for q in range(n) if q >= L and q not in hb]
         t = np.arange(p["num_tiles"], dtype=np.int64)
         G = deposit(t, rest)[:, None] | deposit(e, list(range(L)) + hb)[None, :]
         T = st[G]
         for blk in plan["blocks"][p["block_begin"]:p["block_begin"] + p["num_blocks"]]:
-            idx = deposit(np.arange(256, dtype=np.int64), blk["rows"])[:, None] | \
+            idx = deposit(np.arange(1 << (tb - 5), dtype=np.int64), blk["rows"][:tb - 5])[:, None] | \
                 deposit(np.arange(32, dtype=np.int64), blk["pos"])[None, :]
             U = block_unitary(imgs[blk["image"]])
             T[:, idx] = T[:, idx] @ U.T
@@ -76,11 +81,14 @@ def test_fused_plan_replays_the_circuit(n, depth):
     g = mixed_circuit(n, depth, 0xF0 + n)
     plan = fused_plan(g, n)
     assert len(plan["blocks"]) > 0 and all(p["num_blocks"] > 0 for p in plan["passes"])
+    tb = tile_bits(plan["passes"][0])
+    assert tb in (12, 13)
     for b in plan["blocks"]:
-        assert sorted(b["pos"] + b["rows"]) == list(range(13))
+        assert sorted(b["pos"] + b["rows"][:tb - 5]) == list(range(tb))
     for p in plan["passes"]:
         L = p["num_low"]
-        assert len(set(p["hbits"])) == 13 - L and min(p["hbits"]) >= L and max(p["hbits"]) < n
+        assert tile_bits(p) == tb
+        assert len(set(p["hbits"])) == tb - L and min(p["hbits"]) >= L and max(p["hbits"]) < n
     init = np.zeros(1 << n, dtype=np.complex128)
     init[0] = 1
     got = replay(plan, n, init)
@@ -93,4 +101,4 @@ def test_fused_plan_replays_the_circuit(n, depth):
 def test_fused_plan_rejects_wide_ops_and_small_states():
     from moonlab_b200._lib import MlbError
     with pytest.raises(MlbError):
-        fused_plan(brickwork(12, 2, 1), 12)
+        fused_plan(brickwork(11, 2, 1), 11)

@@ -52,16 +52,16 @@ def test_fused_fidelity_vs_oracle(gpu, n, depth):
 
 
 def test_fused_mode_falls_back_to_tile_passes(gpu):
-    """complex128 states refuse the fused mode; a complex64 state under 13
-    qubits, and an op on more than 5 qubits inside a fused circuit, run as
-    tile passes in order with the fused blocks."""
+    """complex128 states refuse the fused mode; a complex64 state smaller
+    than one tile (11 qubits), and an op on more than 5 qubits inside a fused
+    circuit, run as tile passes in order with the fused blocks."""
     from moonlab_b200._lib import MlbError
     with StateVector(14, "c128") as sv, pytest.raises(MlbError):
         sv.set_exec_mode("fused")
-    g12 = brickwork(12, 6, 3)
-    got, st = run_fused(12, g12)
+    g11 = brickwork(11, 6, 3)
+    got, st = run_fused(11, g11)
     assert st["dense_blocks"] == 0
-    assert np.abs(got - B.port_run(12, g12)).max() < 1e-5
+    assert np.abs(got - B.port_run(11, g11)).max() < 1e-5
     n = 16
     with StateVector(n, "c64") as sv:
         sv.set_exec_mode("fused")
