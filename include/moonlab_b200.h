@@ -282,7 +282,8 @@ void mlb_server_destroy(mlb_server_t *s);
 typedef struct {
     uint64_t passes;
     uint64_t ops;
-    uint64_t dense_blocks;
+    uint64_t dense_blocks;   /* fused complex64 blocks, or complex128 segments run as dense
+                                matrices on the FP64 tensor cores */
     uint64_t bytes_moved;    /* algorithmic HBM bytes of the launched passes */
     uint64_t kernel_launches;
     uint64_t segments;       /* shared-memory register-group round trips over all passes */
@@ -298,6 +299,14 @@ int  mlb_last_flush_stats(mlb_state_t *s, mlb_flush_stats_t *out);
  * one CUDA graph (captured at the shape's first replay).  Results are
  * identical with and without the cache.  0 entries (default) = off. */
 int  mlb_state_set_plan_cache(mlb_state_t *s, size_t entries);
+/* complex128 tiled mode: run each register segment that fits (4 register
+ * qubits in a 13-qubit tile, at most 4 conditioning qubits outside them) as a
+ * dense 16x16 complex matrix on the FP64 tensor cores (mma.sync f64), the
+ * others gate by gate.  On (1) by default; 0 runs every segment gate by gate.
+ * Queued ops are flushed first.  Results agree to rounding (~1e-15 per
+ * amplitude per pass).  No counterpart in the reference, whose CPU path has
+ * no such choice. */
+int  mlb_state_set_dense(mlb_state_t *s, int on);
 /* Record CUDA events around each flush's kernels on the state's stream;
  * mlb_last_flush_stats then reports their elapsed device time (synchronizes). */
 int  mlb_state_set_timing(mlb_state_t *s, int enable);

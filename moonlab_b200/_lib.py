@@ -126,6 +126,7 @@ _SIGS = {
     "mlb_last_flush_stats": (C.c_int, [C.c_void_p, C.POINTER(MlbFlushStats)]),
     "mlb_state_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "mlb_state_set_plan_cache": (C.c_int, [C.c_void_p, C.c_size_t]),
+    "mlb_state_set_dense": (C.c_int, [C.c_void_p, C.c_int]),
     "mlb_plan_ops": (C.c_int, [C.POINTER(MlbOp), C.c_size_t, C.c_uint32, C.c_int, C.c_int,
                                C.POINTER(MlbFlushStats)]),
     "mlb_total_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),

@@ -20,6 +20,7 @@
 #include <string>
 #include <vector>
 
+#include "dense.h"
 #include "fused.h"
 #include "mlb_internal.h"
 #include "planner.h"
@@ -89,6 +90,7 @@ struct mlb_state {
   bool own_stream = true;
   int mode = MLB_EXEC_TILED;
   bool fuse1q = true;
+  bool dense_c128 = true;  // complex128 register segments as dense matrices on the FP64 tensor cores
   int num_sms = 148;
   std::vector<mlb_op_t> queue;
   // device scratch for reductions
@@ -500,21 +502,46 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
     s->plan_hits++;
   }
   E->last_use = ++s->plan_clock;
-  // one upload: ops then segments
+  // complex128: register segments that fit run as dense 16x16 matrices on
+  // the FP64 tensor cores (mode 2), built from this circuit's matrices every
+  // flush; which segments fit depends only on the plan's shape, so the upload
+  // layout (and a captured graph's pointers) repeat with the shape
+  std::vector<DevSegment> dev_segs(E->segs);
+  std::vector<DenseSegDev> dsegs;
+  std::vector<double> frags;
+  if (s->dtype == MLB_C128 && s->dense_c128) {
+    for (const auto& pp : E->passes)
+      for (int k = 0; k < pp.pass.num_segments; k++) {
+        DevSegment& sg = dev_segs[pp.seg_begin + k];
+        const int idx = (int)dsegs.size();
+        if (dense::build_segment(pp.pass, E->segs[pp.seg_begin + k], E->dops.data(), dsegs, frags)) {
+          sg.mode = 2;
+          sg.dense = idx;
+        }
+      }
+  }
+  // one upload: ops, segments, dense segments, dense fragments
   const size_t ob = E->dops.size() * sizeof(DevOp);
-  const size_t sb = E->segs.size() * sizeof(DevSegment);
-  std::vector<unsigned char> blob(ob + sb + 16);
+  const size_t sb = dev_segs.size() * sizeof(DevSegment);
+  const size_t soff = (ob + 15) & ~(size_t)15;
+  const size_t doff = (soff + sb + 15) & ~(size_t)15;
+  const size_t foff = (doff + dsegs.size() * sizeof(DenseSegDev) + 15) & ~(size_t)15;
+  const size_t total = foff + frags.size() * sizeof(double);
+  std::vector<unsigned char> blob(total);
   std::memcpy(blob.data(), E->dops.data(), ob);
-  size_t soff = (ob + 15) & ~(size_t)15;
-  std::memcpy(blob.data() + soff, E->segs.data(), sb);
-  int rc = upload_plan(s, blob.data(), soff + sb);
+  std::memcpy(blob.data() + soff, dev_segs.data(), sb);
+  if (!dsegs.empty()) std::memcpy(blob.data() + doff, dsegs.data(), dsegs.size() * sizeof(DenseSegDev));
+  if (!frags.empty()) std::memcpy(blob.data() + foff, frags.data(), frags.size() * sizeof(double));
+  int rc = upload_plan(s, blob.data(), total);
   if (rc) return rc;
   const DevOp* d_ops = reinterpret_cast<const DevOp*>(s->d_plan);
   const DevSegment* d_segs = reinterpret_cast<const DevSegment*>((unsigned char*)s->d_plan + soff);
+  const DenseSegDev* d_dsegs = reinterpret_cast<const DenseSegDev*>((unsigned char*)s->d_plan + doff);
+  const double* d_frags = reinterpret_cast<const double*>((unsigned char*)s->d_plan + foff);
   auto launch_passes = [&]() -> int {
     for (const auto& pp : E->passes) {
-      int r = launch_tile_pass(s->dtype, s->amp, pp.pass, d_segs + pp.seg_begin, d_ops, nullptr, s->num_sms,
-                               s->stream);
+      const int r = launch_tile_pass(s->dtype, s->amp, pp.pass, d_segs + pp.seg_begin, d_ops, d_dsegs, d_frags,
+                                     s->num_sms, s->stream);
       if (r) return r;
     }
     return MLB_OK;
@@ -555,6 +582,7 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   st.bytes_moved += E->passes.size() * 2 * ab * dim;
   st.ops += ops.size();
   st.segments += E->segs.size();
+  st.dense_blocks += dsegs.size();
   st.plan_cache_hit = hit ? 1 : 0;
   return MLB_OK;
 }
@@ -774,6 +802,24 @@ int mlb_state_stream(const mlb_state_t* s, void** out) {
   *out = (void*)s->stream;
   return MLB_OK;
 }
+int mlb_state_set_dense(mlb_state_t* s, int on) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);  // queued ops keep the setting they were queued under
+  if (rc) return rc;
+  if (s->dense_c128 != (on != 0)) {
+    rc = sync_stream(s);  // cached graphs read the old segment modes; they may still be running
+    if (rc) return rc;
+    for (auto& e : s->plan_cache)
+      if (e.exec) {
+        cudaGraphExecDestroy(e.exec);
+        e.exec = nullptr;
+      }
+  }
+  s->dense_c128 = on != 0;
+  return MLB_OK;
+}
+
 int mlb_state_set_plan_cache(mlb_state_t* s, size_t entries) {
   if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
   DeviceGuard dg(s->device);
@@ -1313,6 +1359,14 @@ int mlb_plan_ops(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fus
   mlb_flush_stats_t st{};
   st.passes = pl.passes.size();
   st.segments = pl.segs.size();
+  if (dtype == MLB_C128) {  // segments that run dense (the default)
+    std::vector<DenseSegDev> dsegs;
+    std::vector<double> frags;
+    for (const auto& pp : pl.passes)
+      for (int k = 0; k < pp.pass.num_segments; k++)
+        dense::build_segment(pp.pass, pl.segs[pp.seg_begin + k], pl.dops.data(), dsegs, frags);
+    st.dense_blocks = dsegs.size();
+  }
   st.ops = fused.size();
   st.kernel_launches = pl.passes.size();
   st.bytes_moved = st.passes * 2ull * (dtype == MLB_C128 ? 16ull : 8ull) * (1ull << n);

@@ -57,7 +57,6 @@ constexpr int kPairsPerThread = kTileAmps / 2 / kFThreads;  // 16
 constexpr uint32_t kBHi = 0;          // 64 rows x 128 B, then lo
 constexpr uint32_t kBLo = 8192;
 constexpr uint32_t kTile0 = 16384;    // one tile buffer of 2^13 float2 (64 KiB)
-constexpr uint32_t kTileBytes = 65536;
 constexpr uint32_t kMbarMma = 81920;  // two: one per 128-row half
 constexpr uint32_t kMbarB = 81936;
 constexpr uint32_t kTmemSlot = 81944;

@@ -18,6 +18,17 @@
 // masks and diagonal keys on qubits outside the tile -- is evaluated once
 // per tile.  Shared memory is XOR-swizzled on 128-byte rows so that group
 // gathers of any stride are bank-conflict free.
+//
+// complex128 segments that the host multiplied into one 16x16 complex matrix
+// (dense.h; mode 2) run on the FP64 tensor cores instead: the tile's 512
+// groups of 16 amplitudes are the columns of a 32 x 512 real block, each warp
+// takes 8 groups at a time (an n = 8 column tile), loads them as the B
+// fragments of 8 k-steps (four 16-byte loads per lane), runs 4 m-tiles x 8
+// k-steps = 32 mma.sync m8n8k4 f64 with the matrix fragments in registers and
+// stores the D fragments back in place (four 16-byte stores per lane).  Gate
+// by gate, a segment's ~12 ops cost about as many FP64 multiply-adds as the
+// dense product (64 per amplitude) but spend two thirds of their instruction
+// issue on addressing, dispatch and register moves; one DMMA is 256 of them.
 #include <atomic>
 #include <cstdio>
 
@@ -176,10 +187,72 @@ __host__ __device__ constexpr int code_pair(int kind, int rt, int ctrl) { return
 __host__ __device__ constexpr int code_swap(int rt, int rt2, int ctrl) { return 64 + (rt * 4 + rt2) * 2 + ctrl; }
 __host__ __device__ constexpr int code_diag(int phase, int ctrl) { return 96 + phase * 2 + ctrl; }
 
+__device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Mode-2 segment: every group of the tile times the segment's dense matrix
+// (the variant of this group's and tile's conditioning bits).  Fragment
+// layout of mma.sync m8n8k4 f64 (lane l, r = l >> 2, c = l & 3): A[r][c],
+// B[c][r], D[r][2 c], D[r][2 c + 1]; the host stores the matrix so that
+// lane l's B operands are whole input slots 4 t + c of group r and its D
+// results whole output slots r and 8 + r of groups 2 c and 2 c + 1.
+template <int NT>
+__device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const DenseSegDev* __restrict__ sg,
+                                              const double* __restrict__ frags, uint64_t tile_base) {
+  constexpr int kWarps = NT / 32, kPerWarp = 64 / kWarps;  // 64 column tiles of 8 groups
+  // warp w takes column tiles kPerWarp w .. + kPerWarp - 1: their conditioning
+  // values (the top group-index bits) rarely change within a warp
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g8 = lane >> 2, q = lane & 3;
+  const int nloc = sg->nloc, nout = sg->nout;
+  uint32_t vout = 0;
+  for (int j = 0; j < nout; j++) vout |= (uint32_t)((tile_base >> sg->obit[j]) & 1ull) << j;
+  uint32_t boff[4];
+#pragma unroll
+  for (int t4 = 0; t4 < 4; t4++) boff[t4] = sg->amp_off[4 * t4 + q];
+  const uint32_t doff0 = sg->amp_off[g8], doff1 = sg->amp_off[8 + g8];
+  const uint32_t glb = sg->g_lo[g8], gld0 = sg->g_lo[2 * q], gld1 = sg->g_lo[2 * q + 1];
+  const double* fseg = frags + sg->frag_off + lane;
+  int cur = -1;
+  double a[32];
+#pragma unroll 1
+  for (int u = 0; u < kPerWarp; u++) {
+    const int j = kPerWarp * warp + u;  // column tile: groups 8 j .. 8 j + 7
+    const uint32_t ghi = sg->g_hi[j];
+    const int var = (nloc ? (j >> (6 - nloc)) : 0) | (int)(vout << nloc);
+    if (var != cur) {  // warp-uniform
+      const double* f = fseg + (size_t)var * 1024;
+#pragma unroll
+      for (int k = 0; k < 32; k++) a[k] = __ldg(f + 32 * k);
+      cur = var;
+    }
+    double2 x[4];
+#pragma unroll
+    for (int t4 = 0; t4 < 4; t4++) x[t4] = sm[ghi ^ glb ^ boff[t4]];
+    double d[4][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++) d[i][0] = d[i][1] = 0.0;
+#pragma unroll
+    for (int sk = 0; sk < 8; sk++) {
+      const double b = (sk & 1) ? x[sk >> 1].y : x[sk >> 1].x;
+#pragma unroll
+      for (int i = 0; i < 4; i++) dmma_f64(d[i][0], d[i][1], a[i * 8 + sk], b);
+    }
+    // in place: this warp's 8 groups are read above and by no other warp
+    sm[ghi ^ gld0 ^ doff0] = make_double2(d[0][0], d[1][0]);
+    sm[ghi ^ gld0 ^ doff1] = make_double2(d[2][0], d[3][0]);
+    sm[ghi ^ gld1 ^ doff0] = make_double2(d[0][1], d[1][1]);
+    sm[ghi ^ gld1 ^ doff1] = make_double2(d[2][1], d[3][1]);
+  }
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
     k_tile(typename Cplx<Real>::T* __restrict__ amp, const DevPass pass,
-           const DevSegment* __restrict__ segs, const DevOp* __restrict__ ops) {
+           const DevSegment* __restrict__ segs, const DevOp* __restrict__ ops,
+           const DenseSegDev* __restrict__ dsegs, const double* __restrict__ frags) {
   using A = typename Cplx<Real>::T;
   constexpr int NT = TileCfg<Real>::NT, RB = TileCfg<Real>::RB, G = 1 << RB, kGPT = TileCfg<Real>::GPT;
   constexpr int TB = TileCfg<Real>::TB;
@@ -278,6 +351,13 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
 
     for (int s = 0; s < nseg; s++) {
       const DevSegment& seg = ssegs[s];
+      if constexpr (sizeof(Real) == 8) {
+        if (seg.mode == 2) {
+          dense_segment<NT>(reinterpret_cast<double2*>(sm), dsegs + seg.dense, frags, tile_base);
+          __syncthreads();
+          continue;
+        }
+      }
       if (seg.mode == 1) {
         const int o = seg.op_begin;
         if (ton[o]) smem_quad<Real>(sm, tile_amps, ops[op0 + o], NT);
@@ -383,7 +463,7 @@ void prepare_tile_t() {
 
 template <typename Real>
 int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, const DevOp* d_ops,
-                  int num_sms, cudaStream_t stream) {
+                  const DenseSegDev* d_dsegs, const double* d_frags, int num_sms, cudaStream_t stream) {
   using A = typename Cplx<Real>::T;
   constexpr int NT = TileCfg<Real>::NT;
   const size_t smem = sizeof(A) << (pass.L + pass.H);
@@ -393,7 +473,8 @@ int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, cons
   if (per_sm < 1) per_sm = 1;
   uint64_t grid = (uint64_t)num_sms * per_sm;
   if (grid > pass.num_tiles) grid = pass.num_tiles;
-  k_tile<Real><<<(unsigned)grid, NT, smem, stream>>>(reinterpret_cast<A*>(amp), pass, d_segs, d_ops);
+  k_tile<Real><<<(unsigned)grid, NT, smem, stream>>>(reinterpret_cast<A*>(amp), pass, d_segs, d_ops, d_dsegs,
+                                                     d_frags);
   count_launch();
   return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
 }
@@ -406,11 +487,12 @@ void prepare_tile_launch(int dtype) {
 }
 
 int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment* d_segs,
-                     const DevOp* d_ops, const float2* d_mats, int num_sms, cudaStream_t stream) {
-  (void)d_mats;
+                     const DevOp* d_ops, const DenseSegDev* d_dsegs, const double* d_frags, int num_sms,
+                     cudaStream_t stream) {
   if (pass.num_segments < 1 || pass.num_segments > kMaxPassSegs) return MLB_ERR_INVALID_ARG;
-  if (dtype == MLB_C128) return launch_tile_t<double>(amp, pass, d_segs, d_ops, num_sms, stream);
-  return launch_tile_t<float>(amp, pass, d_segs, d_ops, num_sms, stream);
+  if (dtype == MLB_C128)
+    return launch_tile_t<double>(amp, pass, d_segs, d_ops, d_dsegs, d_frags, num_sms, stream);
+  return launch_tile_t<float>(amp, pass, d_segs, d_ops, nullptr, nullptr, num_sms, stream);
 }
 
 }  // namespace mlb

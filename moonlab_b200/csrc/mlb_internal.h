@@ -50,7 +50,9 @@ struct DevSegment {
   int32_t op_begin, op_end;
   int32_t nbits;        // number of active register bits (<= R)
   int32_t bits[4];      // local bit positions of the register bits (ascending)
-  int32_t mode;         // 0: register groups; 1: one generic 4x4 op applied in shared memory
+  int32_t mode;         // 0: register groups; 1: one generic 4x4 op applied in shared memory;
+                        // 2: dense 16x16 matrix (complex128) of the ops [op_begin, op_end)
+  int32_t dense;        // mode 2: index into the program's dense segments
 };
 
 constexpr int kMaxHigh = 16;
@@ -68,6 +70,30 @@ struct DevPass {
   uint64_t num_tiles;   // 2^(n - L - H)
   uint64_t tile_free_mask; // global bits that enumerate tiles (not in the tile)
 };
+
+// ---- dense complex128 segments (dense.h, kernels_tile.cu) ----
+// A register segment of a complex128 tile pass applied as one 16x16 complex
+// matrix on its 4 register qubits, on the FP64 tensor cores (mma.sync m8n8k4
+// f64).  The matrix may depend on up to kDenseMaxCond conditioning qubits
+// outside the register set (controls or diagonal keys; tile-local ones vary
+// by group, outside ones by tile): one matrix variant per value of those
+// bits.  Offsets are in 16-byte tile elements, already swizzled (the tile
+// swizzle is linear over GF(2)).
+constexpr int kDenseMaxCond = 4;
+struct DenseSegDev {
+  uint32_t frag_off;   // first double of variant 0 in the fragment pool (1024 per variant)
+  uint8_t nloc;        // tile-local conditioning qubits: group-index bits 9 - nloc .. 8
+  uint8_t nout;        // outside conditioning qubits: global bits obit[0 .. nout)
+  uint8_t pad[2];
+  uint8_t obit[4];
+  uint16_t amp_off[16];  // fragment slot a -> offset
+  uint16_t g_lo[8];      // group-index bits 0..2 -> offset
+  uint16_t g_hi[64];     // group-index bits 3..8 -> offset
+  uint32_t pad2;
+};
+// Swizzle of a complex128 tile in shared memory (16-byte elements, 8 per
+// 128-byte row): linear over GF(2), a bijection.
+__host__ __device__ inline uint32_t tile_swz16(uint32_t e) { return e ^ ((e >> 3) & 7u); }
 
 // ---------------------------------------------------------------------------
 // Adjoint-gradient passes (kernels_adjoint.cu).  A pass covers a batch of
@@ -116,8 +142,11 @@ int launch_adj_reduce(const double* d_partials, uint64_t tiles_per_state, int nu
                       const int* d_param_of_slot, int num_params, double* d_out, cudaStream_t stream);
 
 // Kernel launchers (kernels_*.cu).  All asynchronous on `stream`.
+// d_dsegs / d_frags: the program's dense segments and their matrix fragments
+// (complex128 segments of mode 2; may be null when there are none).
 int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment* d_segs,
-                     const DevOp* d_ops, const float2* d_mats, int num_sms, cudaStream_t stream);
+                     const DevOp* d_ops, const DenseSegDev* d_dsegs, const double* d_frags, int num_sms,
+                     cudaStream_t stream);
 // Sets the tile kernel's function attributes on the current device (done
 // lazily by launch_tile_pass; called before a stream capture).
 void prepare_tile_launch(int dtype);

@@ -107,6 +107,11 @@ class StateVector:
     def set_plan_cache(self, entries: int) -> None:
         check(self._lib.mlb_state_set_plan_cache(self._h, entries), "mlb_state_set_plan_cache")
 
+    def set_dense(self, on: bool = True) -> None:
+        """complex128 tiled mode: segments as dense matrices on the FP64
+        tensor cores where they fit (default), or every segment gate by gate."""
+        check(self._lib.mlb_state_set_dense(self._h, 1 if on else 0), "mlb_state_set_dense")
+
     def set_timing(self, enable: bool = True) -> None:
         check(self._lib.mlb_state_set_timing(self._h, 1 if enable else 0), "mlb_state_set_timing")
 
