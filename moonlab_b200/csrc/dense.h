@@ -61,7 +61,8 @@ inline bool conditioning(const DevSegment& sg, const DevOp* ops, uint32_t& condl
     condout |= d.ocmask | d.omask;
   }
   condloc &= ~reg;
-  return popc32(condloc) + popc64(condout) <= kDenseMaxCond;
+  return popc32(condloc) <= kDenseMaxCondLoc && popc64(condout) <= kDenseMaxCondOut &&
+         popc32(condloc) + popc64(condout) <= kDenseMaxCond;
 }
 
 // One op applied to a 16-slot vector x (slots in sg.bits order); locv: the
@@ -133,38 +134,43 @@ inline void apply(const DevOp& d, const DevSegment& sg, uint32_t locv, uint64_t 
   }
 }
 
-// Dense form of one segment of pass P: appends its dense segment and
-// fragments and returns true, or returns false (appending nothing).
-inline bool build_segment(const DevPass& P, const DevSegment& sg, const DevOp* ops,
-                          std::vector<DenseSegDev>& dsegs, std::vector<double>& frags) {
+// Per-segment data that the fragment fill needs besides the segment itself.
+struct SegPlan {
+  int locbits[kDenseMaxCondLoc];
+  int kappa[16];  // fragment slot -> matrix slot (register qubits in sg.bits order)
+  int nvar;
+};
+
+// Tables of one segment of pass P (everything but the matrices).  False when
+// the segment does not fit.
+inline bool plan_segment(const DevPass& P, const DevSegment& sg, const DevOp* ops, DenseSegDev& D, SegPlan& S) {
   uint32_t cl = 0;
   uint64_t co = 0;
   if (P.L + P.H != 13 || !conditioning(sg, ops, cl, co)) return false;
-  DenseSegDev D;
   std::memset(&D, 0, sizeof D);
   uint32_t reg = 0;
   for (int b = 0; b < 4; b++) reg |= 1u << sg.bits[b];
-  int locbits[kDenseMaxCond], nloc = 0, nout = 0;
+  int nloc = 0, nout = 0;
   for (int b = 0; b < 13; b++)
-    if (cl >> b & 1u) locbits[nloc++] = b;
+    if (cl >> b & 1u) S.locbits[nloc++] = b;
   for (int b = 0; b < 64; b++)
     if (co >> b & 1ull) D.obit[nout++] = (uint8_t)b;
   D.nloc = (uint8_t)nloc;
   D.nout = (uint8_t)nout;
+  S.nvar = 1 << (nloc + nout);
 
   // Bank groups: a 16-byte access lands in bank group = low 3 bits of
-  // tile_swz16(e), to which tile bit p adds bit p mod 3 (p < 6) or nothing.
-  // An 8-lane phase of the B loads varies fragment slot bits 0, 1 and group
-  // bit 0; one of the D stores varies slot bit 0 and group bits 1, 2.  Choose
-  // the slot order (fragment slot bit i = register qubit perm[i]) and the
-  // first three group bits so that those bits reach distinct bank-group bits.
-  auto ub = [](int p) { return p >= 0 && p < 6 ? 1 << (p % 3) : 0; };
+  // tile_swz16(e), to which tile bit p adds bit p mod 3.  An 8-lane phase of
+  // the B loads varies fragment slot bits 0, 1 and group bit 0; one of the D
+  // stores varies slot bit 0 and group bits 1, 2.  Choose the slot order
+  // (fragment slot bit i = register qubit perm[i]) and the first three group
+  // bits so that those bits reach distinct bank-group bits.
+  auto ub = [](int p) { return p >= 0 ? 1 << (p % 3) : 0; };
   int perm[4] = {0, 1, 2, 3};
   bool found = false;
   for (int i = 0; i < 4 && !found; i++)
-    for (int j = i + 1; j < 4 && !found; j++) {
-      const int ui = ub(sg.bits[i]), uj = ub(sg.bits[j]);
-      if (ui && uj && ui != uj) {
+    for (int j = i + 1; j < 4 && !found; j++)
+      if (ub(sg.bits[i]) != ub(sg.bits[j])) {
         int rest = 2;
         perm[0] = i;
         perm[1] = j;
@@ -172,7 +178,6 @@ inline bool build_segment(const DevPass& P, const DevSegment& sg, const DevOp* o
           if (k != i && k != j) perm[rest++] = k;
         found = true;
       }
-    }
   // group-index bits: three chosen free bits, the other free local bits, then
   // the conditioning ones (a run of 8 groups shares its conditioning values)
   int free_bits[9], nfree = 0;
@@ -181,7 +186,7 @@ inline bool build_segment(const DevPass& P, const DevSegment& sg, const DevOp* o
   bool used[9] = {false, false, false, false, false, false, false, false, false};
   auto pick = [&](int avoid) {  // a free bit whose bank-group bit is outside `avoid`
     for (int i = 0; i < nfree; i++)
-      if (!used[i] && ub(free_bits[i]) && !(ub(free_bits[i]) & avoid)) { used[i] = true; return free_bits[i]; }
+      if (!used[i] && !(ub(free_bits[i]) & avoid)) { used[i] = true; return free_bits[i]; }
     for (int i = 0; i < nfree; i++)
       if (!used[i]) { used[i] = true; return free_bits[i]; }
     return -1;  // not reached: at least 5 free bits
@@ -194,7 +199,7 @@ inline bool build_segment(const DevPass& P, const DevSegment& sg, const DevOp* o
   int ng = 3;
   for (int i = 0; i < nfree; i++)
     if (!used[i]) gbits[ng++] = free_bits[i];
-  for (int i = 0; i < nloc; i++) gbits[ng++] = locbits[i];
+  for (int i = 0; i < nloc; i++) gbits[ng++] = S.locbits[i];
 
   for (int c = 0; c < 8; c++) {
     uint32_t e = 0;
@@ -208,27 +213,29 @@ inline bool build_segment(const DevPass& P, const DevSegment& sg, const DevOp* o
       if (h >> i & 1) e |= 1u << gbits[3 + i];
     D.g_hi[h] = (uint16_t)tile_swz16(e);
   }
-  int kappa[16];  // fragment slot -> matrix slot (register qubits in sg.bits order)
   for (int a = 0; a < 16; a++) {
     uint32_t e = 0;
-    kappa[a] = 0;
+    S.kappa[a] = 0;
     for (int i = 0; i < 4; i++)
       if (a >> i & 1) {
         e |= 1u << sg.bits[perm[i]];
-        kappa[a] |= 1 << perm[i];
+        S.kappa[a] |= 1 << perm[i];
       }
     D.amp_off[a] = (uint16_t)tile_swz16(e);
   }
+  return true;
+}
 
-  D.frag_off = (uint32_t)frags.size();
-  const int nv = 1 << (nloc + nout);
-  for (int v = 0; v < nv; v++) {
+// The matrices of a planned segment: S.nvar variants of 1024 doubles at out.
+inline void fill_fragments(const DevSegment& sg, const DevOp* ops, const DenseSegDev& D, const SegPlan& S,
+                           double* out) {
+  for (int v = 0; v < S.nvar; v++) {
     uint32_t locv = 0;
     uint64_t tb = 0;
-    for (int i = 0; i < nloc; i++)
-      if (v >> i & 1) locv |= 1u << locbits[i];
-    for (int j = 0; j < nout; j++)
-      if (v >> (nloc + j) & 1) tb |= 1ull << D.obit[j];
+    for (int i = 0; i < D.nloc; i++)
+      if (v >> i & 1) locv |= 1u << S.locbits[i];
+    for (int j = 0; j < D.nout; j++)
+      if (v >> (D.nloc + j) & 1) tb |= 1ull << D.obit[j];
     cd U[16][16];  // U[out][in], matrix slots
     for (int c = 0; c < 16; c++) {
       cd x[16];
@@ -236,18 +243,28 @@ inline bool build_segment(const DevPass& P, const DevSegment& sg, const DevOp* o
       for (int o = sg.op_begin; o < sg.op_end; o++) apply(ops[o], sg, locv, tb, x);
       for (int k = 0; k < 16; k++) U[k][c] = x[k];
     }
-    const size_t base = frags.size();
-    frags.resize(base + 1024);
+    double* f = out + (size_t)v * 1024;
     for (int i = 0; i < 4; i++)
       for (int sk = 0; sk < 8; sk++)
         for (int l = 0; l < 32; l++) {
           const int ao = 8 * (i >> 1) + (l >> 2), co_ = i & 1;
           const int ai = 4 * (sk >> 1) + (l & 3), ci = sk & 1;
-          const cd u = U[kappa[ao]][kappa[ai]];
-          const double val = co_ == 0 ? (ci == 0 ? u.real() : -u.imag()) : (ci == 0 ? u.imag() : u.real());
-          frags[base + (size_t)(i * 8 + sk) * 32 + l] = val;
+          const cd u = U[S.kappa[ao]][S.kappa[ai]];
+          f[(i * 8 + sk) * 32 + l] = co_ == 0 ? (ci == 0 ? u.real() : -u.imag()) : (ci == 0 ? u.imag() : u.real());
         }
   }
+}
+
+// Dense form of one segment of pass P: appends its dense segment and
+// fragments and returns true, or returns false (appending nothing).
+inline bool build_segment(const DevPass& P, const DevSegment& sg, const DevOp* ops,
+                          std::vector<DenseSegDev>& dsegs, std::vector<double>& frags) {
+  DenseSegDev D;
+  SegPlan S;
+  if (!plan_segment(P, sg, ops, D, S)) return false;
+  D.frag_off = (uint32_t)frags.size();
+  frags.resize(frags.size() + (size_t)S.nvar * 1024);
+  fill_fragments(sg, ops, D, S, frags.data() + D.frag_off);
   dsegs.push_back(D);
   return true;
 }

@@ -16,8 +16,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "dense.h"
@@ -508,15 +510,23 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   // layout (and a captured graph's pointers) repeat with the shape
   std::vector<DevSegment> dev_segs(E->segs);
   std::vector<DenseSegDev> dsegs;
-  std::vector<double> frags;
+  std::vector<dense::SegPlan> dplans;
+  std::vector<int> dsrc;  // segment of each dense segment
+  size_t nfrag = 0;
   if (s->dtype == MLB_C128 && s->dense_c128) {
     for (const auto& pp : E->passes)
       for (int k = 0; k < pp.pass.num_segments; k++) {
-        DevSegment& sg = dev_segs[pp.seg_begin + k];
-        const int idx = (int)dsegs.size();
-        if (dense::build_segment(pp.pass, E->segs[pp.seg_begin + k], E->dops.data(), dsegs, frags)) {
-          sg.mode = 2;
-          sg.dense = idx;
+        const int si = pp.seg_begin + k;
+        DenseSegDev D;
+        dense::SegPlan S;
+        if (dense::plan_segment(pp.pass, E->segs[si], E->dops.data(), D, S)) {
+          D.frag_off = (uint32_t)nfrag;
+          nfrag += (size_t)S.nvar * 1024;
+          dev_segs[si].mode = 2;
+          dev_segs[si].dense = (int)dsegs.size();
+          dsegs.push_back(D);
+          dplans.push_back(S);
+          dsrc.push_back(si);
         }
       }
   }
@@ -526,13 +536,29 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   const size_t soff = (ob + 15) & ~(size_t)15;
   const size_t doff = (soff + sb + 15) & ~(size_t)15;
   const size_t foff = (doff + dsegs.size() * sizeof(DenseSegDev) + 15) & ~(size_t)15;
-  const size_t total = foff + frags.size() * sizeof(double);
-  std::vector<unsigned char> blob(total);
-  std::memcpy(blob.data(), E->dops.data(), ob);
-  std::memcpy(blob.data() + soff, dev_segs.data(), sb);
-  if (!dsegs.empty()) std::memcpy(blob.data() + doff, dsegs.data(), dsegs.size() * sizeof(DenseSegDev));
-  if (!frags.empty()) std::memcpy(blob.data() + foff, frags.data(), frags.size() * sizeof(double));
-  int rc = upload_plan(s, blob.data(), total);
+  const size_t total = foff + nfrag * sizeof(double);
+  std::unique_ptr<unsigned char[]> blob(new unsigned char[total]);
+  std::memset(blob.get(), 0, foff);
+  std::memcpy(blob.get(), E->dops.data(), ob);
+  std::memcpy(blob.get() + soff, dev_segs.data(), sb);
+  if (!dsegs.empty()) {
+    std::memcpy(blob.get() + doff, dsegs.data(), dsegs.size() * sizeof(DenseSegDev));
+    // the segment matrices, in parallel over segments (~1 ms of host time each
+    // for 64 variants)
+    double* fr = reinterpret_cast<double*>(blob.get() + foff);
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+      for (size_t k; (k = next.fetch_add(1)) < dsegs.size();)
+        dense::fill_fragments(E->segs[dsrc[k]], E->dops.data(), dsegs[k], dplans[k], fr + dsegs[k].frag_off);
+    };
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nth = std::min<size_t>({hw, (size_t)16, 1 + nfrag / (256 * 1024)});
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nth; t++) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+  }
+  int rc = upload_plan(s, blob.get(), total);
   if (rc) return rc;
   const DevOp* d_ops = reinterpret_cast<const DevOp*>(s->d_plan);
   const DevSegment* d_segs = reinterpret_cast<const DevSegment*>((unsigned char*)s->d_plan + soff);

@@ -17,7 +17,8 @@
 // precision), and the tile-constant part of every op -- controls, phase
 // masks and diagonal keys on qubits outside the tile -- is evaluated once
 // per tile.  Shared memory is XOR-swizzled on 128-byte rows so that group
-// gathers of any stride are bank-conflict free.
+// gathers of most strides are bank-conflict free (complex128: every tile bit
+// moves the bank group; see tile_swz16).
 //
 // complex128 segments that the host multiplied into one 16x16 complex matrix
 // (dense.h; mode 2) run on the FP64 tensor cores instead: the tile's 512
@@ -50,6 +51,7 @@ template <> struct TileCfg<float> {   // complex64: 2^13 amps = 64 KiB per CTA
 
 template <typename Real>
 __device__ __forceinline__ uint32_t swz(uint32_t e) {
+  if constexpr (sizeof(Real) == 8) return tile_swz16(e);  // shared with the dense segments' host tables
   return e ^ ((e >> TileCfg<Real>::SW_SHIFT) & TileCfg<Real>::SW_MASK);
 }
 
@@ -217,10 +219,13 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
   const double* fseg = frags + sg->frag_off + lane;
   int cur = -1;
   double a[32];
+  // two column tiles per step: 8 independent accumulator chains per warp
+  // cover the DMMA latency; they differ only in bit 0 of j, so they share
+  // their conditioning values (nloc <= 4 uses bits >= 2)
 #pragma unroll 1
-  for (int u = 0; u < kPerWarp; u++) {
-    const int j = kPerWarp * warp + u;  // column tile: groups 8 j .. 8 j + 7
-    const uint32_t ghi = sg->g_hi[j];
+  for (int u = 0; u < kPerWarp; u += 2) {
+    const int j = kPerWarp * warp + u;  // column tiles j, j + 1: groups 8 j .. 8 j + 15
+    const uint32_t ghi0 = sg->g_hi[j], ghi1 = sg->g_hi[j + 1];
     const int var = (nloc ? (j >> (6 - nloc)) : 0) | (int)(vout << nloc);
     if (var != cur) {  // warp-uniform
       const double* f = fseg + (size_t)var * 1024;
@@ -228,23 +233,34 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
       for (int k = 0; k < 32; k++) a[k] = __ldg(f + 32 * k);
       cur = var;
     }
-    double2 x[4];
+    double2 x0[4], x1[4];
 #pragma unroll
-    for (int t4 = 0; t4 < 4; t4++) x[t4] = sm[ghi ^ glb ^ boff[t4]];
-    double d[4][2];
+    for (int t4 = 0; t4 < 4; t4++) {
+      x0[t4] = sm[ghi0 ^ glb ^ boff[t4]];
+      x1[t4] = sm[ghi1 ^ glb ^ boff[t4]];
+    }
+    double d0[4][2], d1[4][2];
 #pragma unroll
-    for (int i = 0; i < 4; i++) d[i][0] = d[i][1] = 0.0;
+    for (int i = 0; i < 4; i++) d0[i][0] = d0[i][1] = d1[i][0] = d1[i][1] = 0.0;
 #pragma unroll
     for (int sk = 0; sk < 8; sk++) {
-      const double b = (sk & 1) ? x[sk >> 1].y : x[sk >> 1].x;
+      const double b0 = (sk & 1) ? x0[sk >> 1].y : x0[sk >> 1].x;
+      const double b1 = (sk & 1) ? x1[sk >> 1].y : x1[sk >> 1].x;
 #pragma unroll
-      for (int i = 0; i < 4; i++) dmma_f64(d[i][0], d[i][1], a[i * 8 + sk], b);
+      for (int i = 0; i < 4; i++) {
+        dmma_f64(d0[i][0], d0[i][1], a[i * 8 + sk], b0);
+        dmma_f64(d1[i][0], d1[i][1], a[i * 8 + sk], b1);
+      }
     }
-    // in place: this warp's 8 groups are read above and by no other warp
-    sm[ghi ^ gld0 ^ doff0] = make_double2(d[0][0], d[1][0]);
-    sm[ghi ^ gld0 ^ doff1] = make_double2(d[2][0], d[3][0]);
-    sm[ghi ^ gld1 ^ doff0] = make_double2(d[0][1], d[1][1]);
-    sm[ghi ^ gld1 ^ doff1] = make_double2(d[2][1], d[3][1]);
+    // in place: this warp's 16 groups are read above and by no other warp
+    sm[ghi0 ^ gld0 ^ doff0] = make_double2(d0[0][0], d0[1][0]);
+    sm[ghi0 ^ gld0 ^ doff1] = make_double2(d0[2][0], d0[3][0]);
+    sm[ghi0 ^ gld1 ^ doff0] = make_double2(d0[0][1], d0[1][1]);
+    sm[ghi0 ^ gld1 ^ doff1] = make_double2(d0[2][1], d0[3][1]);
+    sm[ghi1 ^ gld0 ^ doff0] = make_double2(d1[0][0], d1[1][0]);
+    sm[ghi1 ^ gld0 ^ doff1] = make_double2(d1[2][0], d1[3][0]);
+    sm[ghi1 ^ gld1 ^ doff0] = make_double2(d1[0][1], d1[1][1]);
+    sm[ghi1 ^ gld1 ^ doff1] = make_double2(d1[2][1], d1[3][1]);
   }
 }
 

@@ -79,7 +79,9 @@ struct DevPass {
 // by group, outside ones by tile): one matrix variant per value of those
 // bits.  Offsets are in 16-byte tile elements, already swizzled (the tile
 // swizzle is linear over GF(2)).
-constexpr int kDenseMaxCond = 4;
+constexpr int kDenseMaxCond = 6;     // conditioning qubits in all (64 variants)
+constexpr int kDenseMaxCondLoc = 4;  // of them tile-local (a warp's 8 column tiles share 1..2 variants)
+constexpr int kDenseMaxCondOut = 4;  // of them outside the tile
 struct DenseSegDev {
   uint32_t frag_off;   // first double of variant 0 in the fragment pool (1024 per variant)
   uint8_t nloc;        // tile-local conditioning qubits: group-index bits 9 - nloc .. 8
@@ -92,8 +94,12 @@ struct DenseSegDev {
   uint32_t pad2;
 };
 // Swizzle of a complex128 tile in shared memory (16-byte elements, 8 per
-// 128-byte row): linear over GF(2), a bijection.
-__host__ __device__ inline uint32_t tile_swz16(uint32_t e) { return e ^ ((e >> 3) & 7u); }
+// 128-byte row): bits 0..2 (the bank group) xor the fold of all higher bits
+// in 3-bit chunks, so every tile bit p moves the bank group (by bit p mod 3).
+// Linear over GF(2) and a bijection (bits >= 3 are unchanged).
+__host__ __device__ inline uint32_t tile_swz16(uint32_t e) {
+  return e ^ (((e >> 3) ^ (e >> 6) ^ (e >> 9) ^ (e >> 12)) & 7u);
+}
 
 // ---------------------------------------------------------------------------
 // Adjoint-gradient passes (kernels_adjoint.cu).  A pass covers a batch of
