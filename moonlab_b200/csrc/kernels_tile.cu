@@ -333,6 +333,14 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   }
   __syncthreads();
 
+  // Full tiles: the store of a tile and the load of the CTA's next tile share
+  // one loop: each thread stores an element from its shared-memory slot and
+  // refills that slot with the next tile's element by a 16/8-byte cp.async
+  // (its own slot, read before, so no barrier), so the load latency overlaps
+  // the stores instead of following them.
+  const bool full = tile_amps == (1u << TB);
+  const uint32_t sm_base = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
+  bool prefetched = false;
   for (uint64_t tile = blockIdx.x; tile < pass.num_tiles; tile += gridDim.x) {
     const uint64_t tile_base = pdep64(tile, pass.tile_free_mask);
     // tile-constant op predicates and keys
@@ -347,7 +355,9 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
     }
     // HBM -> shared (coalesced rows of 2^L amplitudes).  A full tile has a
     // compile-time trip count, so all of a thread's loads are in flight at once.
-    if (tile_amps == (1u << TB)) {
+    if (prefetched) {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    } else if (full) {
       constexpr int PER = (1 << TB) / NT;
       A tmp[PER];
 #pragma unroll
@@ -443,14 +453,32 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
       __syncthreads();
     }
 
-    // shared -> HBM (streaming stores: the state is far larger than L2)
-    if (tile_amps == (1u << TB)) {
+    // shared -> HBM (streaming stores: the state is far larger than L2), and
+    // the next tile's loads into the slots just read
+    if (full) {
       constexpr int PER = (1 << TB) / NT;
-#pragma unroll
+      const uint64_t next = tile + gridDim.x;
+      prefetched = next < pass.num_tiles;
+      const uint64_t next_base = prefetched ? pdep64(next, pass.tile_free_mask) : 0;
+#pragma unroll 8
       for (int j = 0; j < PER; j++) {
         const uint32_t e = threadIdx.x + j * NT;
-        __stcs(&amp[tile_base | rowoff[e >> L] | (e & lmask_low)], sm[swz<Real>(e)]);
+        const uint32_t slot = swz<Real>(e);
+        const uint64_t off = rowoff[e >> L] | (e & lmask_low);
+        const A v = sm[slot];
+        __stcs(&amp[tile_base | off], v);  // consumes v: the slot has been read
+        if (prefetched) {
+          if constexpr (sizeof(A) == 16)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sm_base + slot * 16u),
+                         "l"(&amp[next_base | off])
+                         : "memory");
+          else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sm_base + slot * 8u),
+                         "l"(&amp[next_base | off])
+                         : "memory");
+        }
       }
+      if (prefetched) asm volatile("cp.async.commit_group;\n" ::: "memory");
     } else {
       for (uint32_t e = threadIdx.x; e < tile_amps; e += NT) {
         const uint64_t gidx = tile_base | rowoff[e >> L] | (e & lmask_low);
