@@ -28,14 +28,16 @@
 // of half w >> 2, one tile row per thread) holds one tile buffer, the
 // block's operand image and 256 TMEM columns, so two CTAs share an SM: one
 // CTA's MMA waits and tile loads (16-byte async copies, cp.async) overlap
-// the other's operand conversion and readback.  A half's MMAs start as soon
-// as its own four warps have stored their rows (a named barrier per half),
-// and the two halves are issued from different SM sub-partitions: one thread
-// issues an MMA only every ~70 cycles, so one issuer alone would leave the
-// tensor core half idle at N = 64.  MMA descriptors are precomputed (the
-// per-MMA part is a constant add).  Each block's operand image comes by one
-// bulk copy completing on its own mbarrier, requested as soon as both
-// halves' MMAs have completed.
+// the other's operand conversion and readback.  A tile's loads are issued
+// from the previous tile's store loop, into the slots just stored, so they
+// overlap the stores.  A half's MMAs start as soon as its own four warps
+// have stored their rows (a named barrier per half), and the two halves are
+// issued from different SM sub-partitions: one thread issues an MMA only
+// every ~70 cycles, so one issuer alone would leave the tensor core half idle
+// at N = 64.  MMA descriptors are precomputed (the per-MMA part is a
+// constant add).  Each block's operand image comes by one bulk copy
+// completing on its own mbarrier, requested as soon as both halves' MMAs
+// have completed.
 //
 // Waits are bounded: if one runs out the kernel sets *err, waits once more
 // (bounded) for what it issued, frees its tensor memory and returns.
@@ -270,16 +272,19 @@ __global__ void __launch_bounds__(kFThreads, 2)
   if (tid == 0 && (uint64_t)blockIdx.x < pass.num_tiles)
     bulk_load(sbase + kBHi, images + (size_t)imgtab[0] * 16384, 16384, bar_b);
   float2* tile = reinterpret_cast<float2*>(sm + kTile0);
+  // A tile's loads are issued by the previous tile's store loop (each thread
+  // refills the 16-byte slots it has just stored), except for the first tile.
+  bool prefetched = false;
   for (uint64_t t = blockIdx.x; t < pass.num_tiles && !bad; t += gridDim.x) {
-    {
+    if (!prefetched) {
       const uint64_t gb = tile_base(t, tmask) | my_off;
       const uint32_t dst0 = sbase + kTile0;
 #pragma unroll 8
       for (int i = 0; i < kPairsPerThread; i++)
         cp_async16(dst0 + (my_sw0 ^ tsw((uint32_t)i * 2u * kFThreads)) * 8u, amp + (gb | hidep[i]));
       asm volatile("cp.async.commit_group;\n" ::: "memory");
-      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
 
     for (uint32_t b = 0; b < pass.num_blocks; b++) {
@@ -390,16 +395,24 @@ __global__ void __launch_bounds__(kFThreads, 2)
     }
     if (bad) break;
 
-    // store
+    // store, and the next tile's loads into the slots just read (this
+    // thread's own slots, read before: no barrier needed in between)
     {
       const uint64_t gb = tile_base(t, tmask) | my_off;
+      const uint64_t next = t + gridDim.x;
+      prefetched = next < pass.num_tiles;
+      const uint64_t ngb = prefetched ? (tile_base(next, tmask) | my_off) : 0;
+      const uint32_t dst0 = sbase + kTile0;
 #pragma unroll 8
       for (int i = 0; i < kPairsPerThread; i++) {
-        const float4 v = *reinterpret_cast<const float4*>(tile + (my_sw0 ^ tsw((uint32_t)i * 2u * kFThreads)));
-        __stcs(reinterpret_cast<float4*>(amp + (gb | hidep[i])), v);
+        const uint32_t slot = my_sw0 ^ tsw((uint32_t)i * 2u * kFThreads);
+        const float4 v = *reinterpret_cast<const float4*>(tile + slot);
+        __stcs(reinterpret_cast<float4*>(amp + (gb | hidep[i])), v);  // consumes v: the slot has been read
+        if (prefetched) cp_async16(dst0 + slot * 8u, amp + (ngb | hidep[i]));
       }
+      if (prefetched) asm volatile("cp.async.commit_group;\n" ::: "memory");
     }
-    __syncthreads();  // the tile buffer is free for the next load
+    __syncthreads();
   }
 
   // leave no async copy or MMA in flight
