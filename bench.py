@@ -49,6 +49,12 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# FP64 tensor-core (mma.sync m8n8k4 f64) peak of one B200 as measured here:
+# 63.5 multiply-adds per clock per SM with 8 independent accumulator chains
+# per warp and 8+ warps per SM, x 148 SMs x 2 flops x 1.965 GHz.
+DMMA_PEAK_TFLOPS = 36.9
+
+
 def profiled_traffic(n: int):
     """DRAM bytes of one k_tile<double> pass at n qubits: the ncu figure of
     bytes per amplitude (profiles/k_tile_c128_26q.md, dram read + write of
@@ -252,10 +258,14 @@ def run_b200(args, ws, rank, local):
     t_max = dist_max(t, ws)
     st = sv.flush_stats()
     passes = int(st["passes"])
+    dense_segments = int(st["dense_blocks"])
     per_pass_bytes = 2 * 16 * (1 << n)
     avg_pass_s = statistics.median(pass_ms) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = per_pass_bytes / avg_pass_s / 1e9
+    # the dense segments' FP64 tensor-core work: a 16x16 complex matrix on
+    # every 16 amplitudes = 64 real multiply-adds (128 flops) per amplitude
+    dense_flops = dense_segments * 128.0 * (1 << n)
 
     # end to end through the C ABI: host gate records in, <Z_i> + 1024 shots out
     e2e_t = []
@@ -348,6 +358,13 @@ def run_b200(args, ws, rank, local):
                          "frac": achieved / peak, "traffic": profiled_traffic(n),
                          "kernel": "k_tile<double>", "peak_source": peak_kind,
                          "algorithmic_bytes_per_pass": per_pass_bytes},
+            # what bounds the c128 pass now: the FP64 tensor pipe (mma.sync f64)
+            # running the dense segments; peak = DMMA_PEAK_TFLOPS (see there)
+            "fp64_tensor": {"dense_segments": dense_segments, "segments": int(st["segments"]),
+                            "flops_per_circuit": dense_flops,
+                            "achieved_tflops": dense_flops / t_max / 1e12,
+                            "peak_tflops": DMMA_PEAK_TFLOPS,
+                            "frac_of_circuit_time": dense_flops / t_max / 1e12 / DMMA_PEAK_TFLOPS},
             "c64": c64,
             "fused_c64": fused,
             "e2e": {"value": replicas.job_throughput(1.0, ws, e2e_s), "unit": "circuits/s",
