@@ -189,6 +189,8 @@ __host__ __device__ constexpr int code_pair(int kind, int rt, int ctrl) { return
 __host__ __device__ constexpr int code_swap(int rt, int rt2, int ctrl) { return 64 + (rt * 4 + rt2) * 2 + ctrl; }
 __host__ __device__ constexpr int code_diag(int phase, int ctrl) { return 96 + phase * 2 + ctrl; }
 
+static_assert(kDenseMaxCondLoc <= 5, "dense segments: a column-tile pair (j, j + 1) must share its variant");
+
 __device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(d0), "+d"(d1)
@@ -221,7 +223,7 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
   double a[32];
   // two column tiles per step: 8 independent accumulator chains per warp
   // cover the DMMA latency; they differ only in bit 0 of j, so they share
-  // their conditioning values (nloc <= 4 uses bits >= 2)
+  // their conditioning values (the top nloc <= 5 of j's 6 bits)
 #pragma unroll 1
   for (int u = 0; u < kPerWarp; u += 2) {
     const int j = kPerWarp * warp + u;  // column tiles j, j + 1: groups 8 j .. 8 j + 15

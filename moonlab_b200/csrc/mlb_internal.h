@@ -80,18 +80,17 @@ struct DevPass {
 // bits.  Offsets are in 16-byte tile elements, already swizzled (the tile
 // swizzle is linear over GF(2)).
 constexpr int kDenseMaxCond = 6;     // conditioning qubits in all (64 variants)
-constexpr int kDenseMaxCondLoc = 4;  // of them tile-local (a warp's 8 column tiles share 1..2 variants)
-constexpr int kDenseMaxCondOut = 4;  // of them outside the tile
+constexpr int kDenseMaxCondLoc = 5;  // of them tile-local (the top group-index bits; a column-tile pair shares one)
+constexpr int kDenseMaxCondOut = 6;  // of them outside the tile
 struct DenseSegDev {
   uint32_t frag_off;   // first double of variant 0 in the fragment pool (1024 per variant)
   uint8_t nloc;        // tile-local conditioning qubits: group-index bits 9 - nloc .. 8
   uint8_t nout;        // outside conditioning qubits: global bits obit[0 .. nout)
   uint8_t pad[2];
-  uint8_t obit[4];
+  uint8_t obit[8];
   uint16_t amp_off[16];  // fragment slot a -> offset
   uint16_t g_lo[8];      // group-index bits 0..2 -> offset
   uint16_t g_hi[64];     // group-index bits 3..8 -> offset
-  uint32_t pad2;
 };
 // Swizzle of a complex128 tile in shared memory (16-byte elements, 8 per
 // 128-byte row): bits 0..2 (the bank group) xor the fold of all higher bits
