@@ -290,6 +290,12 @@ __global__ void __launch_bounds__(kFThreads, 2)
     for (uint32_t b = 0; b < pass.num_blocks; b++) {
       const uint32_t ebase = rowtab[b * 32u + (tid & 15)] ^ rowtab[b * 32u + 16u + ((uint32_t)tid >> 4)];
       const uint4* ct = reinterpret_cast<const uint4*>(coltab + b * 32u);
+      // When tile bit 0 is the block's lowest bit, columns 2k and 2k + 1 are
+      // adjacent amplitudes (offsets differ in bit 0 only; the swizzle keeps
+      // pairs together): move each pair as one 16-byte access.  Otherwise all
+      // of a warp's rows would hit one bank pair per column (tile bit 0 is
+      // the only bit that sets a float2's half of its 16-byte bank group).
+      const bool pairs = (coltab[b * 32u] ^ coltab[b * 32u + 1u]) == 1u;
       // Amplitude operand, row m = tid, in two groups of 16 columns r: word j
       // holds K elements 2j, 2j+1 (re of r for K < 32, im of r - 32 above),
       // hi and lo parts; group g fills words 8g..8g+7 of each quarter.
@@ -301,8 +307,20 @@ __global__ void __launch_bounds__(kFThreads, 2)
 #pragma unroll
           for (int c = 0; c < 4; c++) {  // columns 16 g + 4 c .. + 3
             const uint4 o = ct[4 * g + c];
-            const float2 a0 = tile[ebase ^ o.x], a1 = tile[ebase ^ o.y];
-            const float2 a2 = tile[ebase ^ o.z], a3 = tile[ebase ^ o.w];
+            float2 a0, a1, a2, a3;
+            if (pairs) {  // block-uniform
+              const float4 p0 = *reinterpret_cast<const float4*>(tile + (ebase ^ o.x));
+              const float4 p1 = *reinterpret_cast<const float4*>(tile + (ebase ^ o.z));
+              a0 = make_float2(p0.x, p0.y);
+              a1 = make_float2(p0.z, p0.w);
+              a2 = make_float2(p1.x, p1.y);
+              a3 = make_float2(p1.z, p1.w);
+            } else {
+              a0 = tile[ebase ^ o.x];
+              a1 = tile[ebase ^ o.y];
+              a2 = tile[ebase ^ o.z];
+              a3 = tile[ebase ^ o.w];
+            }
             const __nv_bfloat162 h0 = __floats2bfloat162_rn(a0.x, a1.x), h1 = __floats2bfloat162_rn(a0.y, a1.y);
             const __nv_bfloat162 h2 = __floats2bfloat162_rn(a2.x, a3.x), h3 = __floats2bfloat162_rn(a2.y, a3.y);
             const float2 f0 = __bfloat1622float2(h0), f1 = __bfloat1622float2(h1);
@@ -376,10 +394,17 @@ __global__ void __launch_bounds__(kFThreads, 2)
 #pragma unroll
             for (int c = 0; c < 4; c++) {
               const uint4 o = ct[4 * g + c];
-              tile[ebase ^ o.x] = make_float2(dre[4 * c], dim[4 * c]);
-              tile[ebase ^ o.y] = make_float2(dre[4 * c + 1], dim[4 * c + 1]);
-              tile[ebase ^ o.z] = make_float2(dre[4 * c + 2], dim[4 * c + 2]);
-              tile[ebase ^ o.w] = make_float2(dre[4 * c + 3], dim[4 * c + 3]);
+              if (pairs) {
+                *reinterpret_cast<float4*>(tile + (ebase ^ o.x)) =
+                    make_float4(dre[4 * c], dim[4 * c], dre[4 * c + 1], dim[4 * c + 1]);
+                *reinterpret_cast<float4*>(tile + (ebase ^ o.z)) =
+                    make_float4(dre[4 * c + 2], dim[4 * c + 2], dre[4 * c + 3], dim[4 * c + 3]);
+              } else {
+                tile[ebase ^ o.x] = make_float2(dre[4 * c], dim[4 * c]);
+                tile[ebase ^ o.y] = make_float2(dre[4 * c + 1], dim[4 * c + 1]);
+                tile[ebase ^ o.z] = make_float2(dre[4 * c + 2], dim[4 * c + 2]);
+                tile[ebase ^ o.w] = make_float2(dre[4 * c + 3], dim[4 * c + 3]);
+              }
             }
           }
         }
