@@ -276,7 +276,9 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   constexpr int TB = TileCfg<Real>::TB;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A* sm = reinterpret_cast<A*>(smem_raw);
-  __shared__ uint64_t rowoff[1 << (TileCfg<Real>::TB - 5)];
+  // global offsets of the tile's rows (its high-qubit combinations); rows
+  // are at least 2^kLowBitsC128 amplitudes long
+  __shared__ uint64_t rowoff[1 << (TileCfg<Real>::TB - (kLowBitsC128 < 5 ? kLowBitsC128 : 5))];
   __shared__ SmOp sops[kMaxPassOps];
   __shared__ A smat[kMaxPassOps][4];
   __shared__ uint8_t ton[kMaxPassOps];
@@ -536,6 +538,7 @@ int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment
                      const DevOp* d_ops, const DenseSegDev* d_dsegs, const double* d_frags, int num_sms,
                      cudaStream_t stream) {
   if (pass.num_segments < 1 || pass.num_segments > kMaxPassSegs) return MLB_ERR_INVALID_ARG;
+  if (pass.H > 13 - (kLowBitsC128 < 5 ? kLowBitsC128 : 5)) return MLB_ERR_INVALID_ARG;  // row table size
   if (dtype == MLB_C128)
     return launch_tile_t<double>(amp, pass, d_segs, d_ops, d_dsegs, d_frags, num_sms, stream);
   return launch_tile_t<float>(amp, pass, d_segs, d_ops, nullptr, nullptr, num_sms, stream);

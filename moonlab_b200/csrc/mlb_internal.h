@@ -56,6 +56,7 @@ struct DevSegment {
 };
 
 constexpr int kMaxHigh = 16;
+constexpr int kLowBitsC128 = 3;  // contiguous low qubits of a complex128 tile (planner.h)
 // A pass's op program is decoded into shared memory; the planner keeps every
 // pass within these sizes.
 constexpr int kMaxPassOps = 160;

@@ -320,7 +320,10 @@ struct Planner {
   void plan(const std::vector<mlb_op_t>& ops) {
     std::vector<int> rem(ops.size());
     for (size_t i = 0; i < ops.size(); i++) rem[i] = (int)i;
-    const int L = (int)n <= g.TB ? (int)n : 5;
+    // contiguous low qubits of every tile: complex128 keeps 3 (128-byte rows,
+    // still whole cache lines; more room for the high qubits the ops need:
+    // 49 passes instead of 60 for the 30-qubit depth-40 circuit), complex64 5
+    const int L = (int)n <= g.TB ? (int)n : (dtype == MLB_C128 ? kLowBitsC128 : 5);
     while (!rem.empty()) {
       uint64_t SH = 0;
       std::vector<int> taken;

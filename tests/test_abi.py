@@ -108,8 +108,10 @@ def test_planner_groups_the_brickwork_workloads():
     st = plan(g2, 30)
     assert st.passes <= 80                         # vs 4470 sweeps gate by gate
     assert st.bytes_moved == st.passes * 2 * 16 * (1 << 30)
+    assert st.passes <= 55                         # c128: 3 contiguous low qubits per tile
+    assert st.dense_blocks >= 160                  # c128 segments run as dense matrices
     st64 = plan(g2, 30, dtype=1)
-    assert st64.passes <= st.passes
+    assert st64.passes <= 65                       # c64: 5 contiguous low qubits per tile
 
 
 def test_planner_small_state_single_tile():
