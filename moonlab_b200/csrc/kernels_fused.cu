@@ -72,7 +72,9 @@ constexpr uint32_t kSmemUsed = kImgTab + kMaxBlocks * 4;
 constexpr uint32_t kSmemBytes = kSmemUsed + 1024;  // alignment slack
 constexpr uint32_t kTmemCols = 256;  // D: columns 0..127 (64 per half); A: 128..255
 constexpr uint32_t kACol = 128;      // A of half h: hi at kACol + 64 h, lo at kACol + 64 h + 32
-constexpr long long kWaitLimit = 1ll << 22;      // try_wait rounds before giving up
+constexpr long long kWaitLimit = 1ll << 24;       // try_wait rounds before giving up (a backstop)
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // and 2 s of wall time
+constexpr uint32_t kWaitHintNs = 100000;          // suspend-time hint of one try_wait
 
 // instruction descriptor: D = F32, A = B = BF16, both K-major, N = 64, M = 128
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
@@ -123,23 +125,37 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
       : "r"(taddr));
 }
 
+// One try_wait with a suspend-time hint: a thread whose phase has not
+// completed sleeps (up to the hint) until it completes instead of spinning,
+// so waiting lanes do not take issue slots from the warps that work.
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t"
       ".reg .pred P1;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
       "selp.b32 %0, 1, 0, P1;\n\t"
       "}\n"
       : "=r"(ok)
-      : "r"(bar), "r"(parity)
+      : "r"(bar), "r"(parity), "r"(kWaitHintNs)
       : "memory");
   return ok != 0;
 }
 
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded by time: false after kWaitLimitNs without the phase completing.
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-  for (long long i = 0; i < kWaitLimit; i++)
+  if (mbar_try(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (long long i = 0; i < kWaitLimit; i++) {
     if (mbar_try(bar, parity)) return true;
+    if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
+  }
   return false;
 }
 
