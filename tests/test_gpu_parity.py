@@ -150,8 +150,8 @@ def rand_unitary(rng, d):
     return q * (np.diag(r) / np.abs(np.diag(r)))
 
 
-@pytest.mark.parametrize("n,mode,dtype", [(9, "tiled", "c128"), (15, "tiled", "c128"),
-                                          (15, "eager", "c128"), (17, "tiled", "c128"),
+@pytest.mark.parametrize("n,mode,dtype", [(9, "tiled", "c128"), (13, "tiled", "c128"), (15, "tiled", "c128"),
+                                          (15, "eager", "c128"), (17, "tiled", "c128"), (22, "tiled", "c128"),
                                           (15, "tiled", "c64")])
 def test_random_ops_all_kinds(gpu, n, mode, dtype):
     rng = np.random.default_rng(1234 + n)
@@ -196,6 +196,9 @@ def test_random_ops_all_kinds(gpu, n, mode, dtype):
                 sv.mcz(qq)
                 want = np_apply(want, n, "phase", 0, -1, sum(1 << q for q in qq), np.array([-1.0]))
         got = sv.amplitudes()
+        st = sv.flush_stats()
+    if dtype == "c128" and mode == "tiled" and n >= 13:
+        assert st["dense_blocks"] > 0  # some segments ran on the FP64 tensor cores
     tol = TOL if dtype == "c128" else 2e-5
     assert np.abs(got - want).max() < tol
 
