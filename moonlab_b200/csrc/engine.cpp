@@ -404,12 +404,12 @@ int upload_plan(mlb_state* s, const void* host, size_t bytes) {
 }
 
 // Shape of a planned op list: everything the planner's decisions depend on
-// (kind, qubits, controls, and whether a 1-qubit matrix is real), but not
-// the matrix values.  Equal shapes plan identically.
+// (kind, qubits, controls, whether a 1-qubit matrix is real, and the dense
+// setting), but not the matrix values.  Equal shapes plan identically.
 std::vector<uint64_t> plan_shape(const mlb_state* s, const std::vector<mlb_op_t>& ops) {
   std::vector<uint64_t> w;
   w.reserve(2 * ops.size() + 1);
-  w.push_back((uint64_t)s->n | (uint64_t)s->dtype << 8);
+  w.push_back((uint64_t)s->n | (uint64_t)s->dtype << 8 | (uint64_t)s->dense_c128 << 16);
   for (const auto& o : ops) {
     uint64_t real = 0;
     if (o.kind == MLB_OP_1Q) {
@@ -481,6 +481,7 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   }
   if (!hit) {
     Planner pl{s->n, s->dtype, geo(s->dtype)};
+    pl.dense_limits = s->dtype == MLB_C128 && s->dense_c128;
     pl.plan(ops);
     local.dops = std::move(pl.dops);
     local.src = std::move(pl.dop_src);
@@ -1381,6 +1382,7 @@ int mlb_plan_ops(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fus
   }
   std::vector<mlb_op_t> fused = fuse1q ? fuse_1q_runs(q, n) : q;
   Planner pl{n, dtype, geo(dtype)};
+  pl.dense_limits = dtype == MLB_C128;  // as a state plans it by default
   pl.plan(fused);
   mlb_flush_stats_t st{};
   st.passes = pl.passes.size();

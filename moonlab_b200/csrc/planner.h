@@ -52,6 +52,13 @@ struct Planner {
   int dtype;
   Geo g;
   int max_ops = kMaxPassOps;  // ops per pass (the op program lives in shared memory)
+  // complex128 with dense segments: a register segment is closed before an
+  // op that would take its conditioning qubits (controls and diagonal keys
+  // outside its four register bits) past what one dense 16x16 segment holds,
+  // since a segment over the limit runs gate by gate at several times the
+  // cost; a segment is padded with conditioning bits first, and a pass's
+  // unused high slots are filled so that every tile has 13 bits
+  bool dense_limits = false;
   std::vector<PlannedPass> passes;
   std::vector<DevSegment> segs;
   std::vector<DevOp> dops;
@@ -121,19 +128,31 @@ struct Planner {
   // commute when neither's non-diagonal targets touch the other's qubits
   // (controls and diagonal keys commute with each other); an op may only be
   // scheduled once every earlier op it does not commute with is scheduled.
+  //
+  // `cut` (size N) marks the positions in the returned order where a new
+  // segment starts.
   template <typename LocalMask>
   std::vector<int> schedule_segments(const std::vector<mlb_op_t>& ops, const std::vector<int>& taken,
-                                     LocalMask&& local_mask, int RB) {
+                                     LocalMask&& local_mask, int RB, std::vector<char>& cut) {
     const size_t N = taken.size();
     std::vector<uint32_t> T(N), D(N);
+    std::vector<uint64_t> DO(N);
     std::vector<bool> wide(N);
     for (size_t i = 0; i < N; i++) {
       const mlb_op_t& o = ops[taken[i]];
       uint64_t om;
       local_mask(op_targets(o), T[i], om);
-      local_mask(op_qubits(o) & ~op_targets(o), D[i], om);
+      local_mask(op_qubits(o) & ~op_targets(o), D[i], DO[i]);
       wide[i] = o.kind == MLB_OP_2Q;
     }
+    // the dense-segment limits for register bits S, local conditioning
+    // bits Dl and outside ones Do (padding absorbs up to RB - |S| of Dl)
+    auto fits_dense = [&](uint32_t S, uint32_t Dl, uint64_t Do) {
+      const int cl = std::max(0, popc(Dl & ~S) - (RB - popc(S)));
+      const int co = popc(Do);
+      return cl <= kDenseMaxCondLoc && co <= kDenseMaxCondOut && cl + co <= kDenseMaxCond;
+    };
+    cut.assign(N, 0);
     std::vector<int> blockers(N, 0);
     std::vector<std::vector<int>> after(N);
     for (size_t i = 0; i < N; i++)
@@ -153,7 +172,9 @@ struct Planner {
       for (int k : after[i]) blockers[k]--;
     };
     while (out.size() < N) {
-      uint32_t S = 0;
+      cut[out.size()] = 1;
+      uint32_t S = 0, Dl = 0;
+      uint64_t Do = 0;
       bool any = false;
       bool progress = true;
       while (progress) {
@@ -169,8 +190,10 @@ struct Planner {
             }
             continue;
           }
-          if (popc(S | T[i]) <= RB) {
+          if (popc(S | T[i]) <= RB && (!dense_limits || !any || fits_dense(S | T[i], Dl | D[i], Do | DO[i]))) {
             S |= T[i];
+            Dl |= D[i];
+            Do |= DO[i];
             take(i);
             any = true;
             progress = true;
@@ -180,6 +203,13 @@ struct Planner {
       }
     }
     return out;
+  }
+
+  template <typename LocalMask>
+  std::vector<int> schedule_segments(const std::vector<mlb_op_t>& ops, const std::vector<int>& taken,
+                                     LocalMask&& local_mask, int RB) {
+    std::vector<char> cut;
+    return schedule_segments(ops, taken, local_mask, RB, cut);
   }
 
   void lower_pass(const std::vector<mlb_op_t>& ops, const std::vector<int>& taken, int L, uint64_t SH) {
@@ -214,7 +244,8 @@ struct Planner {
           else om |= 1ull << b;
         }
     };
-    const std::vector<int> order = schedule_segments(ops, taken, local_mask, RB);
+    std::vector<char> cut;
+    const std::vector<int> order = schedule_segments(ops, taken, local_mask, RB, cut);
     const std::vector<int>& taken_in = taken;
     (void)taken_in;
     auto run_segments = [&](const std::vector<int>& taken) {
@@ -245,6 +276,7 @@ struct Planner {
       size_t j = i;
       for (; j < taken.size(); j++) {
         if (ops[taken[j]].kind == MLB_OP_2Q) break;
+        if (dense_limits && j > i && cut[j]) break;
         const uint64_t T = op_targets(ops[taken[j]]);
         uint32_t tl = 0;
         uint64_t dummy;
@@ -252,7 +284,21 @@ struct Planner {
         if (popc(bits | tl) > RB) break;
         bits |= tl;
       }
-      // pad to RB bits with the lowest free local bits
+      // pad to RB bits: conditioning bits first (dense segments), then the
+      // lowest free local bits
+      if (dense_limits) {
+        uint32_t cond = 0;
+        for (size_t k = i; k < j; k++) {
+          const mlb_op_t& o = ops[taken[k]];
+          uint32_t lm;
+          uint64_t om;
+          local_mask(op_qubits(o) & ~op_targets(o), lm, om);
+          cond |= lm;
+        }
+        cond &= ~bits;
+        for (int b = 0; b < m && popc(bits) < RB; b++)
+          if (cond >> b & 1u) bits |= 1u << b;
+      }
       for (int b = 0; b < m && popc(bits) < RB; b++) bits |= 1u << b;
       DevSegment sg{};
       sg.nbits = 0;
@@ -331,6 +377,24 @@ struct Planner {
         taken.assign(rem.begin(), rem.begin() + std::min<size_t>(rem.size(), kMaxPassOps));
       } else {
         taken = choose(ops, rem, L, SH);
+        if (dense_limits) {
+          // fill the unused high slots, qubits that condition the pass's
+          // ops first (inside the tile, a segment can take them as
+          // register bits), then the lowest free ones
+          const int Hmax = g.TB - L;
+          const uint64_t inside = SH | ((1ull << L) - 1ull);
+          std::vector<int> cnt(n, 0);
+          for (int idx : taken) {
+            const uint64_t q = op_qubits(ops[idx]) & ~inside;
+            for (uint32_t b = 0; b < n; b++)
+              if (q >> b & 1ull) cnt[b]++;
+          }
+          std::vector<int> order;
+          for (uint32_t b = L; b < n; b++)
+            if (!(inside >> b & 1ull)) order.push_back((int)b);
+          std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cnt[a] > cnt[b]; });
+          for (int k = 0; k < (int)order.size() && popc(SH) < Hmax; k++) SH |= 1ull << order[k];
+        }
       }
       lower_pass(ops, taken, L, SH);
       // remove taken (both lists ascending)

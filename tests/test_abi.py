@@ -109,7 +109,12 @@ def test_planner_groups_the_brickwork_workloads():
     assert st.passes <= 80                         # vs 4470 sweeps gate by gate
     assert st.bytes_moved == st.passes * 2 * 16 * (1 << 30)
     assert st.passes <= 55                         # c128: 3 contiguous low qubits per tile
-    assert st.dense_blocks >= 160                  # c128 segments run as dense matrices
+    # c128: every register segment runs as a dense matrix (segments close
+    # before their conditioning qubits outgrow one; full 13-bit tiles)
+    assert st.dense_blocks == st.segments
+    for n in (16, 22, 26):
+        st = plan(brickwork(n, 40, 0xC2, zz_every=4), n)
+        assert st.dense_blocks == st.segments
     st64 = plan(g2, 30, dtype=1)
     assert st64.passes <= 65                       # c64: 5 contiguous low qubits per tile
 
