@@ -6,9 +6,9 @@
 // conditioning qubits outside them (controls and diagonal keys of its ops,
 // tile-local or outside the tile).  Its ops are multiplied into one 16x16
 // complex matrix per value of the conditioning qubits, in FP64, by applying
-// the ops to the 16 basis vectors with exactly the semantics of the
-// register-group code (kernels_tile.cu: op_pair, op_swap, op_diag and the tile
-// predicates), and the real 32x32 form of each matrix is written in the
+// the ops in turn to the identity (row operations on all 16 columns at once)
+// with exactly the semantics of the register-group code (kernels_tile.cu:
+// op_pair, op_swap, op_diag and the tile predicates), and the real 32x32 form of each matrix is written in the
 // A-fragment order of mma.sync m8n8k4 f64 (row.col):
 //   fragment (i, s), lane l holds A[8 i + (l >> 2)][4 s + (l & 3)],
 //   real row 8 i + r  = component i & 1 (re, im) of output slot 8 (i >> 1) + r,
@@ -19,7 +19,6 @@
 // 16-byte shared-memory access each).  Host-only.
 #pragma once
 
-#include <complex>
 #include <cstring>
 #include <utility>
 #include <vector>
@@ -28,8 +27,6 @@
 
 namespace mlb {
 namespace dense {
-
-using cd = std::complex<double>;
 
 inline int popc32(uint32_t x) { return __builtin_popcount(x); }
 inline int popc64(uint64_t x) { return __builtin_popcountll(x); }
@@ -65,35 +62,48 @@ inline bool conditioning(const DevSegment& sg, const DevOp* ops, uint32_t& condl
          popc32(condloc) + popc64(condout) <= kDenseMaxCond;
 }
 
-// One op applied to a 16-slot vector x (slots in sg.bits order); locv: the
-// conditioning local bits' values (a local mask), tb: the conditioning
-// outside bits' values (global).
-inline void apply(const DevOp& d, const DevSegment& sg, uint32_t locv, uint64_t tb, cd* x) {
+// One op applied to the segment matrix U (U[out][in] over the 16 slots in
+// sg.bits order, real and imaginary parts apart) from the left: the op acts
+// on every column at once.  locs[k]: the tile-local bits of slot k (the
+// variant's conditioning local bits included); tb: the variant's outside
+// bits (global).
+inline void apply_rows(const DevOp& d, const uint32_t* locs, uint64_t tb, double (*Ur)[16], double (*Ui)[16]) {
   if ((tb & d.ocmask) != d.ocmask) return;  // outside controls (tile predicate)
   if (d.kind == DOP_PHASE && (tb & d.omask) != d.omask) return;
-  auto loc = [&](int k) {
-    uint32_t r = locv;
-    for (int b = 0; b < 4; b++)
-      if (k >> b & 1) r |= 1u << sg.bits[b];
-    return r;
+  const double m0r = d.m[0], m0i = d.m[1], m1r = d.m[2], m1i = d.m[3];
+  const double m2r = d.m[4], m2i = d.m[5], m3r = d.m[6], m3i = d.m[7];
+  auto ctrl_ok = [&](int k) { return (locs[k] & d.lcmask) == d.lcmask; };
+  auto scale = [&](int k, double pr, double pi) {
+    for (int c = 0; c < 16; c++) {
+      const double xr = Ur[k][c], xi = Ui[k][c];
+      Ur[k][c] = pr * xr - pi * xi;
+      Ui[k][c] = pr * xi + pi * xr;
+    }
   };
-  auto ctrl_ok = [&](int k) { return (loc(k) & d.lcmask) == d.lcmask; };
-  const cd m0(d.m[0], d.m[1]), m1(d.m[2], d.m[3]), m2(d.m[4], d.m[5]), m3(d.m[6], d.m[7]);
   switch (d.kind) {
     case DOP_1Q_GEN:
     case DOP_1Q_REAL:
     case DOP_X: {
       const int bt = 1 << d.rt;
       for (int k = 0; k < 16; k++) {
-        if (k & bt) continue;
-        if (!ctrl_ok(k)) continue;
-        const cd a0 = x[k], a1 = x[k | bt];
+        if ((k & bt) || !ctrl_ok(k)) continue;
+        double* r0 = Ur[k];
+        double* i0 = Ui[k];
+        double* r1 = Ur[k | bt];
+        double* i1 = Ui[k | bt];
         if (d.kind == DOP_X) {
-          x[k] = a1;
-          x[k | bt] = a0;
-        } else {
-          x[k] = m0 * a0 + m1 * a1;
-          x[k | bt] = m2 * a0 + m3 * a1;
+          for (int c = 0; c < 16; c++) {
+            std::swap(r0[c], r1[c]);
+            std::swap(i0[c], i1[c]);
+          }
+          continue;
+        }
+        for (int c = 0; c < 16; c++) {
+          const double ar = r0[c], ai = i0[c], br = r1[c], bi = i1[c];
+          r0[c] = m0r * ar - m0i * ai + m1r * br - m1i * bi;
+          i0[c] = m0r * ai + m0i * ar + m1r * bi + m1i * br;
+          r1[c] = m2r * ar - m2i * ai + m3r * br - m3i * bi;
+          i1[c] = m2r * ai + m2i * ar + m3r * bi + m3i * br;
         }
       }
       break;
@@ -101,9 +111,11 @@ inline void apply(const DevOp& d, const DevSegment& sg, uint32_t locv, uint64_t 
     case DOP_SWAP: {
       const int b0 = 1 << d.rt, b1 = 1 << d.rt2;
       for (int k = 0; k < 16; k++) {
-        if (k & (b0 | b1)) continue;
-        if (!ctrl_ok(k)) continue;
-        std::swap(x[k | b0], x[k | b1]);
+        if ((k & (b0 | b1)) || !ctrl_ok(k)) continue;
+        for (int c = 0; c < 16; c++) {
+          std::swap(Ur[k | b0][c], Ur[k | b1][c]);
+          std::swap(Ui[k | b0][c], Ui[k | b1][c]);
+        }
       }
       break;
     }
@@ -120,15 +132,16 @@ inline void apply(const DevOp& d, const DevSegment& sg, uint32_t locv, uint64_t 
       const uint32_t tkey = (uint32_t)(popc64(tb & d.omask) & 1);
       for (int k = 0; k < 16; k++) {
         if (!ctrl_ok(k)) continue;
-        const uint32_t l = loc(k);
+        const uint32_t l = locs[k];
         const uint32_t key = ((l >> la) ^ (l >> lb) ^ tkey) & 1u;
-        x[k] *= key ? m1 : m0;
+        if (key) scale(k, m1r, m1i);
+        else scale(k, m0r, m0i);
       }
       break;
     }
     case DOP_PHASE:
       for (int k = 0; k < 16; k++)
-        if ((loc(k) & d.lmask) == d.lmask) x[k] *= m0;
+        if ((locs[k] & d.lmask) == d.lmask) scale(k, m0r, m0i);
       break;
     default: break;
   }
@@ -229,6 +242,33 @@ inline bool plan_segment(const DevPass& P, const DevSegment& sg, const DevOp* op
 // The matrices of a planned segment: S.nvar variants of 1024 doubles at out.
 inline void fill_fragments(const DevSegment& sg, const DevOp* ops, const DenseSegDev& D, const SegPlan& S,
                            double* out) {
+  // the ops before the first one that reads a conditioning bit are the same
+  // for every variant: their product is computed once
+  uint32_t locmask = 0;
+  uint64_t outmask = 0;
+  for (int i = 0; i < D.nloc; i++) locmask |= 1u << S.locbits[i];
+  for (int j = 0; j < D.nout; j++) outmask |= 1ull << D.obit[j];
+  int first_dep = sg.op_begin;
+  for (; first_dep < sg.op_end; first_dep++) {
+    const DevOp& d = ops[first_dep];
+    uint32_t keys = d.lcmask;
+    if (d.kind == DOP_PHASE || d.kind == DOP_ZZ) keys |= d.lmask;
+    if (d.kind == DOP_DIAG1 && d.lt >= 0) keys |= 1u << d.lt;
+    if ((keys & locmask) || ((d.ocmask | d.omask) & outmask)) break;
+  }
+  uint32_t slot_loc[16];  // tile-local bits of each slot (register bits only)
+  for (int k = 0; k < 16; k++) {
+    slot_loc[k] = 0;
+    for (int b = 0; b < 4; b++)
+      if (k >> b & 1) slot_loc[k] |= 1u << sg.bits[b];
+  }
+  double Pr[16][16], Pi[16][16];  // U[out][in] over the matrix slots: the common prefix
+  for (int k = 0; k < 16; k++)
+    for (int c = 0; c < 16; c++) {
+      Pr[k][c] = k == c ? 1.0 : 0.0;
+      Pi[k][c] = 0.0;
+    }
+  for (int o = sg.op_begin; o < first_dep; o++) apply_rows(ops[o], slot_loc, 0, Pr, Pi);
   for (int v = 0; v < S.nvar; v++) {
     uint32_t locv = 0;
     uint64_t tb = 0;
@@ -236,21 +276,20 @@ inline void fill_fragments(const DevSegment& sg, const DevOp* ops, const DenseSe
       if (v >> i & 1) locv |= 1u << S.locbits[i];
     for (int j = 0; j < D.nout; j++)
       if (v >> (D.nloc + j) & 1) tb |= 1ull << D.obit[j];
-    cd U[16][16];  // U[out][in], matrix slots
-    for (int c = 0; c < 16; c++) {
-      cd x[16];
-      for (int k = 0; k < 16; k++) x[k] = k == c ? cd(1.0, 0.0) : cd(0.0, 0.0);
-      for (int o = sg.op_begin; o < sg.op_end; o++) apply(ops[o], sg, locv, tb, x);
-      for (int k = 0; k < 16; k++) U[k][c] = x[k];
-    }
+    uint32_t locs[16];  // tile-local bits of each slot under this variant
+    for (int k = 0; k < 16; k++) locs[k] = slot_loc[k] | locv;
+    double Ur[16][16], Ui[16][16];
+    std::memcpy(Ur, Pr, sizeof Ur);
+    std::memcpy(Ui, Pi, sizeof Ui);
+    for (int o = first_dep; o < sg.op_end; o++) apply_rows(ops[o], locs, tb, Ur, Ui);
     double* f = out + (size_t)v * 1024;
     for (int i = 0; i < 4; i++)
       for (int sk = 0; sk < 8; sk++)
         for (int l = 0; l < 32; l++) {
           const int ao = 8 * (i >> 1) + (l >> 2), co_ = i & 1;
           const int ai = 4 * (sk >> 1) + (l & 3), ci = sk & 1;
-          const cd u = U[S.kappa[ao]][S.kappa[ai]];
-          f[(i * 8 + sk) * 32 + l] = co_ == 0 ? (ci == 0 ? u.real() : -u.imag()) : (ci == 0 ? u.imag() : u.real());
+          const double ur = Ur[S.kappa[ao]][S.kappa[ai]], ui = Ui[S.kappa[ao]][S.kappa[ai]];
+          f[(i * 8 + sk) * 32 + l] = co_ == 0 ? (ci == 0 ? ur : -ui) : (ci == 0 ? ui : ur);
         }
   }
 }
