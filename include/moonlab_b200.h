@@ -213,6 +213,30 @@ typedef struct {
 } mlb_job_desc_t;
 int  mlb_job_parse_json(const char *json, mlb_job_desc_t *desc, mlb_gate_t *gates,
                         size_t capacity, size_t *num_gates);
+/* Circuit text: the "moonlab-circuit v1" line format of
+ * moonlab_qgtl_circuit_serialize / moonlab_qgtl_circuit_deserialize
+ * (moonlab_qgtl_backend.h:190-205, moonlab_qgtl_backend.c:319-506).
+ * mlb_circuit_parse_text reads it into gate records (types 0..13; for
+ * CNOT/CY/CZ/SWAP the line is "<NAME> <target> <control>") with the
+ * deserializer's rules: len = 0 reads a NUL-terminated string, and with
+ * len > 0 a NUL inside the extent is invalid; "NUM_QUBITS n" (1..32) must
+ * be the first line that is not blank or a '#' comment; a line over 255
+ * bytes, an unknown name, a missing field, a qubit out of range or a
+ * control equal to its target is invalid (MLB_ERR_INVALID_ARG).  Records
+ * of one-qubit gates get control = -1.  Pass gates = NULL to learn the
+ * count; with a buffer that is too small the call returns
+ * MLB_ERR_INVALID_ARG and sets *num_gates to the count needed.
+ * mlb_circuit_format_text writes the serializer's text byte for byte
+ * (theta with %.17g, so it round-trips exactly); a record type without a
+ * name in the format (20..27) gives MLB_ERR_NOT_SUPPORTED.  buf = NULL,
+ * capacity = 0 asks for the length; too small a buffer gives
+ * MLB_ERR_INVALID_ARG with *written = the capacity needed (text + NUL).
+ * Replaces moonlab_qgtl_circuit_deserialize / _serialize (moonlab_qgtl_backend.h:
+ * 227-252) for callers that go straight to mlb_run_gates or mlb_job_run. */
+int  mlb_circuit_parse_text(const char *text, size_t len, uint32_t *num_qubits, mlb_gate_t *gates,
+                            size_t capacity, size_t *num_gates);
+int  mlb_circuit_format_text(uint32_t num_qubits, const mlb_gate_t *gates, size_t num_gates, char *buf,
+                             size_t capacity, size_t *written);
 /* Run a job with the semantics of the scheduler's default "simulator"
  * backend (simulator_backend_execute, scheduler.c:194-239): workers =
  * min(num_workers, num_shots), worker w takes shots [w S / W, (w+1) S / W)

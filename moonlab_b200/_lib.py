@@ -151,6 +151,10 @@ _SIGS = {
                                                   C.POINTER(C.c_double), C.c_size_t]),
     "mlb_job_parse_json": (C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                      C.POINTER(C.c_size_t)]),
+    "mlb_circuit_parse_text": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_uint32), C.c_void_p,
+                                         C.c_size_t, C.POINTER(C.c_size_t)]),
+    "mlb_circuit_format_text": (C.c_int, [C.c_uint32, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t,
+                                          C.POINTER(C.c_size_t)]),
     "mlb_job_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.POINTER(C.c_uint64),
                               C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "moonlab_b200_backend_execute": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -218,6 +218,9 @@ def ref():
             "moonlab_qgtl_add_gate": (i, [C.c_void_p, i, i, i, C.POINTER(d)]),
             "moonlab_qgtl_execute": (i, [C.c_void_p, C.POINTER(QgtlOpts), C.POINTER(QgtlResults)]),
             "moonlab_qgtl_results_free": (None, [C.POINTER(QgtlResults)]),
+            "moonlab_qgtl_circuit_num_gates": (i, [C.c_void_p]),
+            "moonlab_qgtl_circuit_serialize": (i, [C.c_void_p, C.c_char_p, sz, C.POINTER(sz)]),
+            "moonlab_qgtl_circuit_deserialize": (C.c_void_p, [C.c_char_p, sz, C.POINTER(i)]),
             "moonlab_job_create": (C.c_void_p, [i]), "moonlab_job_free": (None, [C.c_void_p]),
             "moonlab_job_add_gate": (i, [C.c_void_p, i, i, i, C.POINTER(d)]),
             "moonlab_job_set_num_shots": (i, [C.c_void_p, i]),
@@ -338,6 +341,49 @@ def ref_qgtl_execute(n: int, gates, shots: int, seed: int, want_probs: bool = Tr
     probs = np.ctypeslib.as_array(res.probabilities, shape=(1 << n,)).copy() if want_probs else None
     L.moonlab_qgtl_results_free(C.byref(res))
     return outs, probs
+
+
+def ref_circuit_serialize(c) -> str:
+    """moonlab_qgtl_circuit_serialize of a reference circuit handle."""
+    L = ref()
+    need = C.c_size_t()
+    rc = L.moonlab_qgtl_circuit_serialize(c, None, 0, C.byref(need))
+    if rc:
+        raise RuntimeError(f"moonlab_qgtl_circuit_serialize: {rc}")
+    buf = C.create_string_buffer(need.value + 1)
+    rc = L.moonlab_qgtl_circuit_serialize(c, buf, len(buf), None)
+    if rc:
+        raise RuntimeError(f"moonlab_qgtl_circuit_serialize: {rc}")
+    return buf.value.decode()
+
+
+def ref_circuit_text(n: int, gates) -> str:
+    """The reference's text for gate records (built with moonlab_qgtl_add_gate)."""
+    L = ref()
+    c = L.moonlab_qgtl_circuit_create(n)
+    try:
+        for g in gates:
+            t, tgt, ctl, th = int(g["type"]), int(g["target"]), int(g["control"]), float(g["theta"])
+            par = C.c_double(th)
+            rc = L.moonlab_qgtl_add_gate(c, t, tgt, ctl, C.byref(par) if t in (7, 8, 9) else None)
+            if rc:
+                raise RuntimeError(f"moonlab_qgtl_add_gate: {rc}")
+        return ref_circuit_serialize(c)
+    finally:
+        L.moonlab_qgtl_circuit_free(c)
+
+
+def ref_circuit_roundtrip(raw: bytes, explicit_len: bool = True):
+    """(status, re-serialized text or None) of moonlab_qgtl_circuit_deserialize."""
+    L = ref()
+    st = C.c_int(0)
+    c = L.moonlab_qgtl_circuit_deserialize(raw, len(raw) if explicit_len else 0, C.byref(st))
+    if not c:
+        return st.value, None
+    try:
+        return st.value, ref_circuit_serialize(c)
+    finally:
+        L.moonlab_qgtl_circuit_free(c)
 
 
 class RefSolver:

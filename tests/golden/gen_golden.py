@@ -6,9 +6,11 @@ library built from its sources (oracle/Makefile -> oracle/_ref/liboracle.so):
 
     make -C oracle ref && python tests/golden/gen_golden.py
 
-Every expected value below is produced by calling the reference's own
-public C functions (gate_*, measurement_*, moonlab_qgtl_execute,
-moonlab_scheduler_run, moonlab_vqe_gradient) through ctypes.
+(`python tests/golden/gen_golden.py circuit_text` writes only
+circuit_text.json.)  Every expected value below is produced by calling the
+reference's own public C functions (gate_*, measurement_*,
+moonlab_qgtl_execute, moonlab_scheduler_run, moonlab_vqe_gradient,
+moonlab_qgtl_circuit_serialize / _deserialize) through ctypes.
 """
 from __future__ import annotations
 
@@ -122,7 +124,86 @@ def main() -> None:
 
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes)")
+    circuit_text()
+
+
+# Edge cases of the "moonlab-circuit v1" reader: the reference's verdict on
+# each (moonlab_qgtl_circuit_deserialize with the text's length).
+TEXT_CASES = [
+    "NUM_QUBITS 4\nH 0\nCNOT 1 0\n",
+    "  # lead comment\n\n\t\nNUM_QUBITS 4\n   # indented comment\nX 3\n\n",
+    "NUM_QUBITS 4\r\nRX 1 0.5\r\nCZ 2 3\r\n",
+    "NUM_QUBITS 4\nRY 0 -1e-300\nRZ 1 1e308\nRX 2 0x1.8p1\nRY 3 +.5\nRZ 0 -0\n",
+    "NUM_QUBITS 4\nRX 0 1e\nRY 1 1e+\nRZ 2 0x1p\n",
+    "NUM_QUBITS 4\nRX 0 inf\nRY 1 -infinity\nRZ 2 nan\n",
+    "NUM_QUBITS 4\nRX 0 0x\n",
+    "NUM_QUBITS 4\nRX 0 infin\n",
+    "NUM_QUBITS 4\nRX 0\n",
+    "NUM_QUBITS 4\nRX 0 .\n",
+    "NUM_QUBITS 4\nH 0 junk after\nCNOT 1 2 3 4\nRX 3 0.25rad\n",
+    "NUM_QUBITS 4\nCNOT 1 1\n",
+    "NUM_QUBITS 4\nCNOT 4 0\n",
+    "NUM_QUBITS 4\nCNOT 0 -1\n",
+    "NUM_QUBITS 4\nCNOT 0\n",
+    "NUM_QUBITS 4\nH 4\n",
+    "NUM_QUBITS 4\nH -1\n",
+    "NUM_QUBITS 4\nH +2\n",
+    "NUM_QUBITS 4\nH 01\n",
+    "NUM_QUBITS 4\nH\n",
+    "NUM_QUBITS 4\nh 0\n",
+    "NUM_QUBITS 4\nCX 0 1\n",
+    "NUM_QUBITS 4\nHADAMARD 0\n",
+    "NUM_QUBITS 4\nH0\n",
+    "NUM_QUBITS 4\nSWAP 3 2\nCY 0 3\nI 1\nS 2\nT 3\nY 0\nZ 1\n",
+    "NUM_QUBITS 4\nCNOT 1+2\n",
+    "NUM_QUBITS 4\nCNOT 1,2\n",
+    "NUM_QUBITS4\nH 0\n",
+    "NUM_QUBITS 4 trailing\nH 0\n",
+    "NUM_QUBITS 0\n",
+    "NUM_QUBITS 32\nH 31\n",
+    "NUM_QUBITS 33\nH 0\n",
+    "NUM_QUBITS -3\n",
+    "NUM_QUBITS\n",
+    "num_qubits 4\nH 0\n",
+    "H 0\nNUM_QUBITS 4\n",
+    "# only a comment\n",
+    "",
+    "NUM_QUBITS 4\nNUM_QUBITS 4\n",
+    "NUM_QUBITS 4",
+    "NUM_QUBITS 4\nRX 3 0.125",
+    "NUM_QUBITS 4\nRX 0 " + "1" * 240 + "\n",
+    "NUM_QUBITS 4\nRX 0 " + "1" * 260 + "\n",
+    "NUM_QUBITS 4\n" + " " * 300 + "\nH 0\n",
+    "NUM_QUBITS 4\n" + " " * 300 + "H 0\n",
+]
+
+
+def circuit_text() -> None:
+    """tests/golden/circuit_text.json: the reference serializer's text for a
+    circuit of every gate type, and its deserializer's verdict on TEXT_CASES."""
+    gates = brickwork(10, 6, 0x7E47)
+    extra = np.zeros(14 + 6, dtype=GATE_DTYPE)
+    extra["type"] = list(range(14)) + [7, 8, 9, 7, 8, 9]
+    extra["target"] = [q % 10 for q in range(3, 23)]
+    extra["control"] = [(q + 4) % 10 for q in range(3, 23)]
+    extra["theta"] = [0.0] * 7 + [1.0 / 3, -2.5, 1e-300] + [0.0] * 4 + [-0.0, 6.283185307179586, 1e300,
+                                                                        float.fromhex("0x1.fffffffffffffp+1"),
+                                                                        5e-324, -12345.678901234567]
+    gates = np.concatenate([gates, extra])
+    text = B.ref_circuit_text(10, gates)
+    cases = []
+    for t in TEXT_CASES:
+        st, back = B.ref_circuit_roundtrip(t.encode())
+        cases.append({"text": t, "status": st, "reserialized": back})
+    out = Path(__file__).resolve().parent / "circuit_text.json"
+    out.write_text(json.dumps({"num_qubits": 10, "gates": [[int(g["type"]), int(g["target"]), int(g["control"]),
+                                                            float(g["theta"]).hex()] for g in gates],
+                               "text": text, "cases": cases}, indent=0))
+    print(f"wrote {out} ({out.stat().st_size} bytes)")
 
 
 if __name__ == "__main__":
+    if sys.argv[1:] == ["circuit_text"]:
+        circuit_text()
+        sys.exit(0)
     main()
