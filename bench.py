@@ -267,6 +267,19 @@ def run_b200(args, ws, rank, local):
     # every 16 amplitudes = 64 real multiply-adds (128 flops) per amplitude
     dense_flops = dense_segments * 128.0 * (1 << n)
 
+    # the same c128 path with dense segments off: every register segment runs
+    # gate by gate on the CUDA cores (no gate matrices multiplied together
+    # beyond runs of 1-qubit gates on one qubit)
+    sv.set_dense(False)
+    gbg = []
+    for i in range(1 + max(1, min(args.steps, 2))):
+        step()
+        st_g = sv.flush_stats()
+        if i > 0:
+            gbg.append(st_g["gpu_ms"] / 1e3)
+    sv.set_dense(True)
+    gbg_s = statistics.median(gbg)
+
     # end to end through the C ABI: host gate records in, <Z_i> + 1024 shots out
     e2e_t = []
     for i in range(max(2, min(args.steps, 3)) + 1):
@@ -317,6 +330,7 @@ def run_b200(args, ws, rank, local):
         per_pass = secs / max(1, st64["passes"])
         gbs = 2 * 8 * (1 << n) / per_pass / 1e9
         return {"circuit_ms": secs * 1e3, "speedup_vs_c128": t_max / secs,
+                "speedup_vs_c128_gate_by_gate": gbg_s / secs,
                 "fidelity": float(ip.abs().item() ** 2) / nb, "norm": nb, "max_amp_err": maxerr,
                 "passes": int(st64["passes"]), "dense_blocks": int(st64["dense_blocks"]),
                 "hbm_gbs_per_pass": gbs, "hbm_frac": gbs / peak}
@@ -365,6 +379,8 @@ def run_b200(args, ws, rank, local):
                             "achieved_tflops": dense_flops / t_max / 1e12,
                             "peak_tflops": DMMA_PEAK_TFLOPS,
                             "frac_of_circuit_time": dense_flops / t_max / 1e12 / DMMA_PEAK_TFLOPS},
+            "c128_gate_by_gate": {"circuit_ms": gbg_s * 1e3, "passes": int(st_g["passes"]),
+                                  "path": "c128 tile passes, dense segments off"},
             "c64": c64,
             "fused_c64": fused,
             "e2e": {"value": replicas.job_throughput(1.0, ws, e2e_s), "unit": "circuits/s",
