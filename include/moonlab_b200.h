@@ -335,7 +335,11 @@ int  mlb_state_set_dense(mlb_state_t *s, int on);
  * mlb_last_flush_stats then reports their elapsed device time (synchronizes). */
 int  mlb_state_set_timing(mlb_state_t *s, int enable);
 /* Plan ops exactly as a flush would, on the host only (no device needed):
- * reports the passes and algorithmic bytes a flush of these ops launches. */
+ * reports the passes and algorithmic bytes a flush of these ops launches.
+ * fuse1q != 0 applies a flush's op fusion first: runs of uncontrolled
+ * 1-qubit ops on one qubit are merged (fusion.c:247-292), and a
+ * CNOT . diagonal . CNOT sandwich on the same (control, target), the
+ * reference's exp(-i g J Z Z) (qaoa.c:598-602), becomes one ZZ op. */
 int  mlb_plan_ops(const mlb_op_t *ops, size_t num_ops, uint32_t num_qubits, int dtype,
                   int fuse1q, mlb_flush_stats_t *out);
 /* The fused complex64 path's plan for these ops, as a flush in MLB_EXEC_FUSED

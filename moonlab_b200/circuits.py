@@ -105,6 +105,28 @@ def brickwork(n: int, depth: int, seed: int, zz_every: int = 0) -> np.ndarray:
     return np.concatenate(layers) if layers else np.zeros(0, dtype=GATE_DTYPE)
 
 
+def qaoa_circuit(n: int, layers: int, seed: int, density: float = 0.3) -> np.ndarray:
+    """QAOA on a random Ising graph, written the way the reference's solver
+    applies it (src/algorithms/qaoa.c:594-602 cost layer, mixer after it):
+    H on every qubit, then per layer CNOT(i, j) . RZ(j, 2 gamma J_ij) . CNOT(i, j)
+    for every edge i < j and RX(q, 2 beta) on every qubit.  Edges (probability
+    `density`), couplings U[-1.5, 1.5) and angles U[0, pi) from SplitMix64(seed)."""
+    u = SplitMix64(seed)
+    edges, J = [], []
+    for i in range(n):
+        for j in range(i + 1, n):
+            if u.uniform() < density:
+                edges.append((i, j))
+                J.append(3.0 * u.uniform() - 1.5)
+    recs = [(GATE_H, q, -1, 0, 0.0) for q in range(n)]
+    for _ in range(layers):
+        gamma, beta = math.pi * u.uniform(), math.pi * u.uniform()
+        for (i, j), jij in zip(edges, J):
+            recs += [(GATE_CNOT, j, i, 0, 0.0), (GATE_RZ, j, -1, 0, 2.0 * gamma * jij), (GATE_CNOT, j, i, 0, 0.0)]
+        recs += [(GATE_RX, q, -1, 0, 2.0 * beta) for q in range(n)]
+    return np.array(recs, dtype=GATE_DTYPE)
+
+
 def config_c1(n: int = 20, depth: int = 20):
     """20-qubit depth-20 brickwork from |0..0>, 1024 shot uniforms."""
     gates = brickwork(n, depth, 0xC1)

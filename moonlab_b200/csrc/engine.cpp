@@ -360,6 +360,53 @@ std::vector<mlb_op_t> fuse_1q_runs(const std::vector<mlb_op_t>& in, uint32_t n) 
   return out;
 }
 
+// X(t | c) . D . X(t | c), with D diagonal on t alone (a DIAG1 on t, or a
+// phase on the |1> half of t) and the same single control c on both X's, is
+// the parity phase d[bit t ^ bit c]: one ZZ op.  Each amplitude is
+// multiplied by the same single diagonal entry as under the three ops (the
+// X's only move amplitudes).  CNOT . RZ . CNOT is how the reference writes
+// exp(-i g J Z Z) in QAOA's cost layer (qaoa.c:598-602, :750-753); as one
+// diagonal op it needs no tile slot for its target.
+std::vector<mlb_op_t> lift_parity_phases(const std::vector<mlb_op_t>& in) {
+  std::vector<mlb_op_t> out;
+  out.reserve(in.size());
+  for (size_t i = 0; i < in.size(); i++) {
+    if (i + 2 < in.size()) {
+      const mlb_op_t &a = in[i], &d = in[i + 1], &b = in[i + 2];
+      const int t = a.target;
+      const bool cx = a.kind == MLB_OP_X && popc(a.cmask) == 1 && b.kind == MLB_OP_X && b.target == t &&
+                      b.cmask == a.cmask;
+      double dm[4];
+      bool diag = false;
+      if (cx && d.kind == MLB_OP_DIAG1 && d.target == t && d.cmask == 0) {
+        std::memcpy(dm, d.m, sizeof dm);
+        diag = true;
+      } else if (cx && d.kind == MLB_OP_PHASE && d.cmask == (1ull << t)) {
+        dm[0] = 1.0; dm[1] = 0.0; dm[2] = d.m[0]; dm[3] = d.m[1];
+        diag = true;
+      }
+      if (diag) {
+        mlb_op_t z{};
+        z.kind = MLB_OP_ZZ;  // amp *= m[0..1] where bit target == bit target2, else m[2..3]
+        z.target = __builtin_ctzll(a.cmask);
+        z.target2 = t;
+        std::memcpy(z.m, dm, sizeof dm);
+        out.push_back(z);
+        i += 2;
+        continue;
+      }
+    }
+    out.push_back(in[i]);
+  }
+  return out;
+}
+
+// The op-level fusion of a flush: 1-qubit runs, then CNOT . diagonal . CNOT
+// sandwiches as parity phases.
+std::vector<mlb_op_t> fuse_ops(const std::vector<mlb_op_t>& in, uint32_t n) {
+  return lift_parity_phases(fuse_1q_runs(in, n));
+}
+
 int ensure_scratch(mlb_state* s, size_t bytes) {
   if (s->scratch_bytes >= bytes) return MLB_OK;
   if (s->d_scratch) {
@@ -641,7 +688,7 @@ int flush_impl(mlb_state* s) {
     s->stats = st;
     return MLB_OK;
   }
-  std::vector<mlb_op_t> ops = s->fuse1q ? fuse_1q_runs(s->queue, s->n) : s->queue;
+  std::vector<mlb_op_t> ops = s->fuse1q ? fuse_ops(s->queue, s->n) : s->queue;
   s->queue.clear();
   if (s->timing) cudaEventRecord(s->t0, s->stream);
   int rc = MLB_OK;
@@ -1361,7 +1408,7 @@ int mlb::prepare_ops(const mlb_gate_t* gates, size_t num, uint32_t n, std::vecto
     if (rc) return rc;
     q.push_back(canonical(raw[i]));
   }
-  out = fuse_1q_runs(q, n);
+  out = fuse_ops(q, n);
   return MLB_OK;
 }
 
@@ -1380,7 +1427,7 @@ int mlb_plan_ops(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fus
     if (rc) return rc;
     q.push_back(canonical(ops[i]));
   }
-  std::vector<mlb_op_t> fused = fuse1q ? fuse_1q_runs(q, n) : q;
+  std::vector<mlb_op_t> fused = fuse1q ? fuse_ops(q, n) : q;
   Planner pl{n, dtype, geo(dtype)};
   pl.dense_limits = dtype == MLB_C128;  // as a state plans it by default
   pl.plan(fused);
@@ -1417,7 +1464,7 @@ int mlb_fused_plan(const mlb_op_t* ops, size_t num, uint32_t n, mlb_fused_pass_t
     if (rc) return rc;
     q.push_back(canonical(ops[i]));
   }
-  std::vector<mlb_op_t> f1 = fuse_1q_runs(q, n);
+  std::vector<mlb_op_t> f1 = fuse_ops(q, n);
   fused::Plan P;
   int rc = fused::plan(f1, n, P);
   if (rc) return fail(rc, "an op spans more than 5 qubits");

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from moonlab_b200 import _lib, gates_to_ops
-from moonlab_b200.circuits import GATE_DTYPE, brickwork, config_c1, config_c2
+from moonlab_b200.circuits import GATE_DTYPE, brickwork, config_c1, config_c2, qaoa_circuit
 
 ROOT = Path(__file__).resolve().parents[1]
 
@@ -117,6 +117,21 @@ def test_planner_groups_the_brickwork_workloads():
         assert st.dense_blocks == st.segments
     st64 = plan(g2, 30, dtype=1)
     assert st64.passes <= 65                       # c64: 5 contiguous low qubits per tile
+
+
+def test_cnot_diagonal_cnot_is_lifted_to_one_zz():
+    # QAOA's cost layer as the reference writes it: each CNOT . RZ . CNOT
+    # becomes one parity-phase op; H and the RX mixer stay single ops
+    g = qaoa_circuit(16, 3, 0x9A0A)
+    edges = int((g["type"] == 9).sum()) // 3
+    st = plan(g, 16)
+    assert st.ops == 16 + 3 * (edges + 16)
+    st0 = plan(g, 16, fuse=0)
+    assert st0.ops == len(g)
+    assert st.passes <= st0.passes
+    # a controlled diagonal, or different controls, is left alone
+    h = np.array([(10, 3, 1, 0, 0.0), (9, 3, -1, 0, 0.7), (10, 3, 2, 0, 0.0)], dtype=GATE_DTYPE)
+    assert plan(h, 6).ops == 3
 
 
 def test_planner_small_state_single_tile():

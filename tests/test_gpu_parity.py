@@ -16,7 +16,7 @@ import pytest
 
 from conftest import corpus_case
 from moonlab_b200 import StateVector, _lib
-from moonlab_b200.circuits import GATE_DTYPE, SplitMix64, brickwork, config_c1
+from moonlab_b200.circuits import GATE_DTYPE, SplitMix64, brickwork, config_c1, qaoa_circuit
 from oracle import bindings as B
 
 pytestmark = pytest.mark.gpu
@@ -107,6 +107,37 @@ def test_brickwork_eager_equals_tiled(gpu):
     with gpu_run(16, g, "tiled") as a, gpu_run(16, g, "eager") as b:
         assert np.abs(a.amplitudes() - b.amplitudes()).max() < TOL
     assert np.abs(B.port_run(16, g) - gpu_run(16, g).amplitudes()).max() < TOL
+
+
+# ---------------------------------------------------------------------------
+# QAOA: CNOT . RZ . CNOT lifted to one parity-phase op per edge
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n,mode,dense", [(12, "tiled", True), (16, "tiled", True), (16, "tiled", False),
+                                          (16, "eager", True), (20, "tiled", True)])
+def test_qaoa_parity_phases(gpu, n, mode, dense):
+    g = qaoa_circuit(n, 3, 0x9A0A ^ n)
+    want = B.port_run(n, g)
+    with StateVector(n, "c128") as sv:
+        sv.set_exec_mode(mode)
+        sv.set_dense(dense)
+        sv.run(g)
+        got = sv.amplitudes()
+        st = sv.flush_stats()
+    assert np.abs(got - want).max() < TOL
+    if mode == "tiled":
+        assert st["ops"] < len(g)  # the sandwiches were lifted
+
+
+def test_qaoa_fused_c64(gpu):
+    n = 16
+    g = qaoa_circuit(n, 3, 0x9A0A ^ n)
+    want = B.port_run(n, g)
+    with StateVector(n, "c64") as sv:
+        sv.set_exec_mode("fused")
+        sv.run(g)
+        got = sv.amplitudes().astype(np.complex128)
+    fid = abs(np.vdot(want, got)) ** 2 / np.vdot(got, got).real
+    assert fid >= 1 - 1e-6
 
 
 # ---------------------------------------------------------------------------
