@@ -302,6 +302,44 @@ int  mlb_server_wait(mlb_server_t *s, uint64_t ticket, int timeout_ms, uint64_t 
 int  mlb_server_get_stats(mlb_server_t *s, mlb_server_stats_t *out);
 void mlb_server_destroy(mlb_server_t *s);
 
+/* ---- control-plane front end ----------------------------------------------
+ * The request execution of the reference's control server
+ * (src/control/control_plane.c:598-770) on the device loop: one request
+ * frame in (the bytes after the AUTH line, if any; the transport, TLS,
+ * AUTH/HMAC, rate limits, METRICS and admission hooks stay the server's),
+ * its response frame out (control_plane.h:8-33):
+ *   "HEALTH\n"                        -> "OK alive\n"
+ *   "CIRCUIT <N>\n" + N bytes of text -> "OK <2^n>\n" + 2^n little-endian
+ *       doubles, re*re + im*im of the output state (moonlab_qgtl_backend.c:199-210)
+ *   "SHOTS <k> <N>\n" + N bytes       -> "SAMPLES <k>\n" + k little-endian
+ *       uint64 outcomes drawn as moonlab_qgtl_execute draws them
+ *   failure                           -> "ERR <code> <message>\n" with the
+ *       reference's codes and messages (-401 out of range, -404 malformed
+ *       frame, -405 rejected: "deserialize" / "execute").
+ * The text is "moonlab-circuit v1" (mlb_circuit_parse_text); limits as the
+ * reference's: body 1..4 MiB, shots 1..2^20, and a qubit cap
+ * (MOONLAB_CONTROL_MAX_QUBITS there): max_qubits, 0 = 30 (the reference's
+ * ceiling; its default is 24), at most 33.  SHOTS requests run in a
+ * continuous-batching server (mlb_server_*, created at the first SHOTS
+ * request with hbm_budget_bytes and num_workers) in complex128, so many
+ * overlap on the device; CIRCUIT requests run one at a time on a complex128
+ * state of their own, outside the server's budget.  Shots take their seed
+ * from the clock, as the reference's server does, unless
+ * mlb_control_set_seed gave a fixed non-zero one (then outcomes equal
+ * moonlab_qgtl_execute's with that seed).  mlb_control_handle is
+ * thread-safe; it returns MLB_OK whenever it produced a response frame (ERR
+ * frames included) in *response (free with mlb_control_free).  No
+ * counterpart in the reference's C API: it is the body of its connection
+ * handler. */
+typedef struct mlb_control mlb_control_t;
+int  mlb_control_create(int device, size_t hbm_budget_bytes, int num_workers, uint32_t max_qubits,
+                        mlb_control_t **out);
+int  mlb_control_set_seed(mlb_control_t *c, uint64_t seed);
+int  mlb_control_handle(mlb_control_t *c, const void *request, size_t request_len, void **response,
+                        size_t *response_len);
+void mlb_control_free(void *response);
+void mlb_control_destroy(mlb_control_t *c);
+
 /* Plan statistics of the last flush: passes launched and ops applied. */
 typedef struct {
     uint64_t passes;

@@ -5,6 +5,8 @@ worker threads admit requests as worker slots and HBM budget free up, so
 requests that arrive while others run overlap with them on the device.
 `run_load` replays a Poisson request stream (circuits.config_c5) against a
 server in real time and reports throughput and latency percentiles.
+`ControlFrontEnd` puts the reference control server's request frames
+(HEALTH / CIRCUIT / SHOTS) onto the same loop.
 """
 from __future__ import annotations
 
@@ -102,6 +104,45 @@ class Server:
         if self._h:
             self._lib.mlb_server_destroy(self._h)
             self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class ControlFrontEnd:
+    """The control server's request execution on the device loop
+    (mlb_control_*): `handle(frame)` takes one request frame of the
+    reference's wire protocol (src/control/control_plane.h:8-33: HEALTH,
+    CIRCUIT <N>, SHOTS <k> <N> with a "moonlab-circuit v1" body) and returns
+    its response frame (OK / SAMPLES / ERR).  SHOTS requests share one
+    continuous-batching server; `set_seed` fixes the shot seed (default: the
+    clock, as the reference's server)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0, workers: int = 8, max_qubits: int = 0):
+        self._lib = _lib.load()
+        self._h = C.c_void_p()
+        check(self._lib.mlb_control_create(device, budget_bytes, workers, max_qubits, C.byref(self._h)),
+              "mlb_control_create")
+
+    def set_seed(self, seed: int) -> None:
+        check(self._lib.mlb_control_set_seed(self._h, seed), "mlb_control_set_seed")
+
+    def handle(self, frame: bytes) -> bytes:
+        out, n = C.c_void_p(), C.c_size_t()
+        check(self._lib.mlb_control_handle(self._h, frame, len(frame), C.byref(out), C.byref(n)),
+              "mlb_control_handle")
+        try:
+            return C.string_at(out, n.value)
+        finally:
+            self._lib.mlb_control_free(out)
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.mlb_control_destroy(self._h)
+            self._h = C.c_void_p()
 
     def __enter__(self):
         return self
