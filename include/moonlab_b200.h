@@ -87,6 +87,11 @@ typedef struct mlb_state mlb_state_t;
 
 /* ---- device / lifecycle ---------------------------------------------- */
 int  mlb_device_count(int *count);
+/* The device's FP64 tensor-core throughput in TFLOP/s, measured now: a
+ * register-only probe of mma.sync m8n8k4 f64 (the instruction of the dense
+ * complex128 segments), 16 warps per SM, best of three launches.  For
+ * rooflines; no counterpart in the reference. */
+int  mlb_fp64_tensor_peak(int device, double *tflops);
 int  mlb_state_create(uint32_t num_qubits, int dtype, int device, mlb_state_t **out);
 void mlb_state_free(mlb_state_t *s);
 int  mlb_state_num_qubits(const mlb_state_t *s, uint32_t *out);

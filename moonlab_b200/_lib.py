@@ -155,6 +155,7 @@ _SIGS = {
                                          C.c_size_t, C.POINTER(C.c_size_t)]),
     "mlb_circuit_format_text": (C.c_int, [C.c_uint32, C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t,
                                           C.POINTER(C.c_size_t)]),
+    "mlb_fp64_tensor_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "mlb_control_create": (C.c_int, [C.c_int, C.c_size_t, C.c_int, C.c_uint32, C.POINTER(C.c_void_p)]),
     "mlb_control_set_seed": (C.c_int, [C.c_void_p, C.c_uint64]),
     "mlb_control_handle": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p),

@@ -773,6 +773,18 @@ int mlb_device_count(int* count) {
   return MLB_OK;
 }
 
+int mlb_fp64_tensor_peak(int device, double* tflops) {
+  if (!tflops) return fail(MLB_ERR_INVALID_ARG, "null out");
+  int cnt = 0;
+  if (mlb_device_count(&cnt) != MLB_OK || device < 0 || device >= cnt) return fail(MLB_ERR_NO_DEVICE, "no such device");
+  DeviceGuard dg(device);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (sms < 1) return fail(MLB_ERR_DRIVER, "multiprocessor count");
+  const int rc = measure_fp64_tensor_peak(sms, tflops);
+  return rc ? fail(rc, "fp64 tensor probe") : MLB_OK;
+}
+
 int mlb_state_create(uint32_t n, int dtype, int device, mlb_state_t** out) {
   if (!out) return fail(MLB_ERR_INVALID_ARG, "null out");
   *out = nullptr;

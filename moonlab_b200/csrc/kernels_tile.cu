@@ -527,7 +527,59 @@ int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, cons
   return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
 }
 
+// FP64 tensor-core throughput probe: 8 independent accumulator chains per
+// warp, as a dense segment runs them, with the operands in registers; the
+// only memory access is one store per thread at the end.
+__global__ void __launch_bounds__(256) k_dmma_probe(double* __restrict__ out, int iters, double a0, double b0) {
+  double d[8][2];
+#pragma unroll
+  for (int i = 0; i < 8; i++) d[i][0] = d[i][1] = 0.0;
+  const double a = a0 + 1e-9 * threadIdx.x, b = b0;
+#pragma unroll 1
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) dmma_f64(d[i][0], d[i][1], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) s += d[i][0] + d[i][1];
+  out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace
+
+int measure_fp64_tensor_peak(int num_sms, double* tflops) {
+  constexpr int kThreads = 256, kIters = 4096, kRuns = 4;
+  const int grid = num_sms * 2;  // 16 warps per SM
+  double* out = nullptr;
+  if (cudaMalloc(&out, sizeof(double) * (size_t)grid * kThreads) != cudaSuccess) return MLB_ERR_OUT_OF_MEMORY;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 0.0f;
+  int rc = MLB_OK;
+  for (int r = 0; r < kRuns && rc == MLB_OK; r++) {  // run 0 warms up
+    cudaEventRecord(e0);
+    k_dmma_probe<<<grid, kThreads>>>(out, kIters, 1e-3, 1e-3);
+    count_launch();
+    cudaEventRecord(e1);
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+      rc = MLB_ERR_DRIVER;
+      break;
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0 && (best == 0.0f || ms < best)) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (rc != MLB_OK) return rc;
+  // one m8n8k4 mma = 8 x 8 x 4 multiply-adds per warp
+  const double flops = 2.0 * 256.0 * 8.0 * kIters * (double)grid * (kThreads / 32);
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return MLB_OK;
+}
 
 void prepare_tile_launch(int dtype) {
   if (dtype == MLB_C128) prepare_tile_t<double>();

@@ -156,6 +156,9 @@ int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment
 // Sets the tile kernel's function attributes on the current device (done
 // lazily by launch_tile_pass; called before a stream capture).
 void prepare_tile_launch(int dtype);
+// The current device's FP64 tensor-core throughput (mma.sync m8n8k4 f64,
+// register operands), best of three timed launches after a warm-up.
+int measure_fp64_tensor_peak(int num_sms, double* tflops);
 int launch_gate(int dtype, void* amp, int n, const mlb_op_t& op, cudaStream_t stream);
 int launch_init_zero(int dtype, void* amp, int n, cudaStream_t stream);
 int launch_convert(int dst_dtype, void* dst, int src_dtype, const void* src, uint64_t dim,

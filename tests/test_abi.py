@@ -65,6 +65,8 @@ def test_no_device_is_reported_not_faked():
     assert lib.quantum_state_create_gpu(10, C.byref(qs)) == -7  # QS_ERROR_NOT_SUPPORTED
     assert not qs
     assert lib.moonlab_cuda_runtime_probe_discrete() in (0, -2)
+    v = C.c_double(-1.0)
+    assert lib.mlb_fp64_tensor_peak(0, C.byref(v)) == -2 and v.value == -1.0  # no probe figure made up
 
 
 def test_gate_matrices_match_host_libm():

@@ -494,3 +494,11 @@ def test_plan_cache_replays_repeated_shapes(gpu):
         a = cached.amplitudes()
         want = B.port_run(n, other)
         assert np.abs(a - want).max() < TOL
+
+
+def test_fp64_tensor_probe(gpu):
+    # the roofline denominator of the dense complex128 segments: a B200 runs
+    # mma.sync f64 at tens of TFLOP/s (nominal FP64 tensor rate about 40)
+    v = C.c_double()
+    assert gpu.mlb_fp64_tensor_peak(0, C.byref(v)) == 0
+    assert 15.0 < v.value < 60.0
