@@ -317,19 +317,28 @@ __global__ void __launch_bounds__(kCT) k_seq_d(const typename Cplx<Real>::T* __r
     __syncthreads();
     while (true) {
       if (threadIdx.x == 0) {
+        // s in binade e is N g with g = 2^(e-52) the binade's grid: N is s's
+        // significand (its mantissa bits with the implicit bit; the raw bits
+        // for a subnormal), and (N + K) g, for N + K < 2^53, has the bit
+        // pattern bits(s) + K (subnormal and normal patterns are contiguous).
+        // So the chain runs on the bit pattern, with no division.
+        unsigned long long b = (unsigned long long)__double_as_longlong(s);
         for (; c < c1; c++) {
-          s_in[c] = s;
-          if (!(s > 0.0)) break;
-          const int e = binade_of(s);
+          s_in[c] = __longlong_as_double((long long)b);
           const Xfer& x = sx[c - c0];
-          const int cand = (x.e[0] == e) ? 0 : (x.e[1] == e) ? 1 : -1;
+          const int xe0 = x.e[0], xe1 = x.e[1];  // independent of s: loaded ahead
+          const long long k00 = x.K[0][0], k01 = x.K[0][1], k10 = x.K[1][0], k11 = x.K[1][1];
+          const int ex = (int)(b >> 52);  // s >= 0: no sign bit
+          if (b == 0ull || ex == 0x7ff) break;  // zero (or inf / nan): replayed
+          const int e = ex ? ex - 1023 : -1023;
+          const int cand = (xe0 == e) ? 0 : (xe1 == e) ? 1 : -1;
           if (cand < 0) break;
-          const double g = grid_of(e);
-          const long long N = (long long)(s / g);
-          const long long K = x.K[cand][(int)(N & 1)];
+          const long long N = ex ? (long long)((b & 0xfffffffffffffull) | 0x10000000000000ull) : (long long)b;
+          const long long K = cand == 0 ? ((b & 1ull) ? k01 : k00) : ((b & 1ull) ? k11 : k10);
           if (N + K >= kTwo53) break;
-          s = (double)(N + K) * g;  // exact: N + K < 2^53
+          b += (unsigned long long)K;
         }
+        s = __longlong_as_double((long long)b);
         s_next = c;
         s_run = s;
       }
