@@ -385,6 +385,36 @@ int  mlb_state_set_timing(mlb_state_t *s, int enable);
  * reference's exp(-i g J Z Z) (qaoa.c:598-602), becomes one ZZ op. */
 int  mlb_plan_ops(const mlb_op_t *ops, size_t num_ops, uint32_t num_qubits, int dtype,
                   int fuse1q, mlb_flush_stats_t *out);
+/* The tile-pass plan a flush of these ops runs (host only), for inspection
+ * and host replay: the ops after op fusion (fuse1q as for mlb_plan_ops) in
+ * execution order, the passes over them and each pass's register-group
+ * segments.  A pass's tile is qubits 0..num_low-1 plus high[0..num_high-1]
+ * (tile bit num_low + i <-> qubit high[i]); every op of the pass has its
+ * non-diagonal targets in the tile, and a mode-0 segment's ops have theirs
+ * among its register bits (tile bits bits[0..nbits-1]).  mode: 0 gate by
+ * gate, 1 one generic 4x4 op in shared memory, 2 a dense 16x16 complex128
+ * matrix on the FP64 tensor cores (dtype MLB_C128 with dense segments on,
+ * as a state flushes by default).  Segments index the ops [op_begin,
+ * op_end) of the execution order.  Call with NULL buffers to learn the
+ * sizes; a buffer too small gives MLB_ERR_INVALID_ARG. */
+typedef struct {
+    uint8_t  high[16];
+    uint8_t  num_low;
+    uint8_t  num_high;
+    uint8_t  reserved[2];
+    uint32_t seg_begin;
+    uint32_t num_segments;
+} mlb_tile_pass_t;
+typedef struct {
+    int32_t  mode;
+    int32_t  nbits;
+    int32_t  bits[4];
+    uint32_t op_begin;
+    uint32_t op_end;
+} mlb_tile_segment_t;
+int  mlb_tile_plan(const mlb_op_t *ops, size_t num_ops, uint32_t num_qubits, int dtype, int fuse1q,
+                   mlb_tile_pass_t *passes, size_t *num_passes, mlb_tile_segment_t *segments,
+                   size_t *num_segments, mlb_op_t *planned_ops, size_t *num_planned);
 /* The fused complex64 path's plan for these ops, as a flush in MLB_EXEC_FUSED
  * mode would launch it (host only).  Passes: tile = qubits 0..num_low-1 plus
  * hbits[0..num_high-1] (tile bit num_low + i <-> hbits[i]); blocks

@@ -54,6 +54,16 @@ class MlbFusedPass(C.Structure):
                 ("num_blocks", C.c_uint32)]
 
 
+class MlbTilePass(C.Structure):
+    _fields_ = [("high", C.c_uint8 * 16), ("num_low", C.c_uint8), ("num_high", C.c_uint8),
+                ("reserved", C.c_uint8 * 2), ("seg_begin", C.c_uint32), ("num_segments", C.c_uint32)]
+
+
+class MlbTileSegment(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("nbits", C.c_int32), ("bits", C.c_int32 * 4), ("op_begin", C.c_uint32),
+                ("op_end", C.c_uint32)]
+
+
 class MlbFusedBlock(C.Structure):
     _fields_ = [("pos", C.c_uint8 * 5), ("rows", C.c_uint8 * 8), ("reserved", C.c_uint8 * 3),
                 ("image", C.c_uint32)]
@@ -130,6 +140,9 @@ _SIGS = {
     "mlb_plan_ops": (C.c_int, [C.POINTER(MlbOp), C.c_size_t, C.c_uint32, C.c_int, C.c_int,
                                C.POINTER(MlbFlushStats)]),
     "mlb_total_kernel_launches": (C.c_int, [C.POINTER(C.c_uint64)]),
+    "mlb_tile_plan": (C.c_int, [C.POINTER(MlbOp), C.c_size_t, C.c_uint32, C.c_int, C.c_int,
+                                C.POINTER(MlbTilePass), C.POINTER(C.c_size_t), C.POINTER(MlbTileSegment),
+                                C.POINTER(C.c_size_t), C.POINTER(MlbOp), C.POINTER(C.c_size_t)]),
     "mlb_fused_plan": (C.c_int, [C.POINTER(MlbOp), C.c_size_t, C.c_uint32, C.POINTER(MlbFusedPass),
                                  C.POINTER(C.c_size_t), C.POINTER(MlbFusedBlock), C.POINTER(C.c_size_t),
                                  C.c_void_p, C.POINTER(C.c_size_t)]),

@@ -1446,18 +1446,76 @@ int mlb_plan_ops(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fus
   mlb_flush_stats_t st{};
   st.passes = pl.passes.size();
   st.segments = pl.segs.size();
-  if (dtype == MLB_C128) {  // segments that run dense (the default)
-    std::vector<DenseSegDev> dsegs;
-    std::vector<double> frags;
+  if (dtype == MLB_C128) {  // segments that run dense (the default); no matrices needed to count them
     for (const auto& pp : pl.passes)
-      for (int k = 0; k < pp.pass.num_segments; k++)
-        dense::build_segment(pp.pass, pl.segs[pp.seg_begin + k], pl.dops.data(), dsegs, frags);
-    st.dense_blocks = dsegs.size();
+      for (int k = 0; k < pp.pass.num_segments; k++) {
+        DenseSegDev D;
+        dense::SegPlan S;
+        if (dense::plan_segment(pp.pass, pl.segs[pp.seg_begin + k], pl.dops.data(), D, S)) st.dense_blocks++;
+      }
   }
   st.ops = fused.size();
   st.kernel_launches = pl.passes.size();
   st.bytes_moved = st.passes * 2ull * (dtype == MLB_C128 ? 16ull : 8ull) * (1ull << n);
   *out = st;
+  return MLB_OK;
+}
+
+int mlb_tile_plan(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fuse1q, mlb_tile_pass_t* passes,
+                  size_t* num_passes, mlb_tile_segment_t* segments, size_t* num_segments, mlb_op_t* planned,
+                  size_t* num_planned) {
+  if ((!ops && num) || !num_passes || !num_segments || !num_planned)
+    return fail(MLB_ERR_INVALID_ARG, "null argument");
+  if (n < 1 || n > 34 || (dtype != MLB_C128 && dtype != MLB_C64)) return fail(MLB_ERR_INVALID_ARG, "bad shape");
+  mlb_state probe;  // host-side only: validation needs n
+  probe.n = n;
+  std::vector<mlb_op_t> q;
+  q.reserve(num);
+  for (size_t i = 0; i < num; i++) {
+    int rc = validate(&probe, ops[i]);
+    if (rc) return rc;
+    q.push_back(canonical(ops[i]));
+  }
+  const std::vector<mlb_op_t> fused = fuse1q ? fuse_ops(q, n) : q;
+  Planner pl{n, dtype, geo(dtype)};
+  pl.dense_limits = dtype == MLB_C128;  // as a state plans it by default
+  pl.plan(fused);
+  const size_t np = pl.passes.size(), ns = pl.segs.size(), no = pl.dops.size();
+  const bool room = (!passes || *num_passes >= np) && (!segments || *num_segments >= ns) &&
+                    (!planned || *num_planned >= no);
+  *num_passes = np;
+  *num_segments = ns;
+  *num_planned = no;
+  if (!room) return fail(MLB_ERR_INVALID_ARG, "plan buffers too small");
+  for (size_t i = 0; passes && i < np; i++) {
+    const PlannedPass& pp = pl.passes[i];
+    mlb_tile_pass_t t{};
+    t.num_low = (uint8_t)pp.pass.L;
+    t.num_high = (uint8_t)pp.pass.H;
+    for (int h = 0; h < pp.pass.H; h++) t.high[h] = (uint8_t)pp.pass.high[h];
+    t.seg_begin = (uint32_t)pp.seg_begin;
+    t.num_segments = (uint32_t)pp.pass.num_segments;
+    passes[i] = t;
+  }
+  for (size_t i = 0; segments && i < np; i++) {
+    const PlannedPass& pp = pl.passes[i];
+    for (int k = pp.seg_begin; k < pp.seg_end; k++) {
+      const DevSegment& sg = pl.segs[k];
+      mlb_tile_segment_t t{};
+      t.mode = sg.mode;
+      if (dtype == MLB_C128) {
+        DenseSegDev D;
+        dense::SegPlan S;
+        if (dense::plan_segment(pp.pass, sg, pl.dops.data(), D, S)) t.mode = 2;
+      }
+      t.nbits = sg.nbits;
+      for (int b = 0; b < 4; b++) t.bits[b] = b < sg.nbits ? sg.bits[b] : -1;
+      t.op_begin = (uint32_t)sg.op_begin;
+      t.op_end = (uint32_t)sg.op_end;
+      segments[k] = t;
+    }
+  }
+  for (size_t k = 0; planned && k < no; k++) planned[k] = fused[pl.dop_src[k]];
   return MLB_OK;
 }
 
