@@ -43,7 +43,8 @@ struct mlb_control {
   uint32_t max_qubits = kDefaultMaxQubits;
   bool fixed_seed = false;
   uint64_t seed = 0;
-  std::mutex mu;               // server creation, CIRCUIT states (one at a time: 2^n probabilities each)
+  std::mutex server_mu;        // creation of the batching server at the first SHOTS request
+  std::mutex circuit_mu;       // CIRCUIT requests run one at a time (a state and 2^n probabilities each)
   mlb_server_t* server = nullptr;
 };
 
@@ -63,7 +64,7 @@ Frame err_frame(int code, const char* msg) {
 int shots_request(mlb_control* c, uint32_t n, const std::vector<mlb_gate_t>& gates, long shots, Frame& out) {
   mlb_server_t* srv = nullptr;
   {
-    std::lock_guard<std::mutex> lk(c->mu);
+    std::lock_guard<std::mutex> lk(c->server_mu);
     if (!c->server && mlb_server_create(c->device, c->hbm_budget, c->num_workers, &c->server) != MLB_OK) {
       out = err_frame(kCtlRejected, "execute");
       return MLB_OK;
@@ -93,7 +94,7 @@ int shots_request(mlb_control* c, uint32_t n, const std::vector<mlb_gate_t>& gat
 }
 
 int circuit_request(mlb_control* c, uint32_t n, const std::vector<mlb_gate_t>& gates, Frame& out) {
-  std::lock_guard<std::mutex> lk(c->mu);
+  std::lock_guard<std::mutex> lk(c->circuit_mu);
   mlb_state_t* s = nullptr;
   const size_t dim = (size_t)1 << n;
   std::vector<uint8_t> probs;
