@@ -236,6 +236,9 @@ def ref():
             "vqe_solver_create": (C.c_void_p, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
             "vqe_solver_free": (None, [C.c_void_p]),
             "moonlab_vqe_gradient": (i, [C.c_void_p, C.POINTER(d), C.POINTER(d), sz]),
+            "moonlab_vqe_qgt": (i, [C.c_void_p, C.POINTER(d), C.POINTER(d), sz]),
+            "moonlab_vqe_berry_curvature": (i, [C.c_void_p, C.POINTER(d), C.POINTER(d), sz]),
+            "vqe_natural_gradient_direction": (i, [C.c_void_p, C.POINTER(d), C.POINTER(d), d, C.POINTER(d)]),
         }
         for name, (res, args) in sigs.items():
             f = getattr(lib, name)
@@ -413,6 +416,31 @@ class RefSolver:
         if rc:
             raise RuntimeError(f"moonlab_vqe_gradient: {rc}")
         return g
+
+    def _tensor(self, fn, params) -> np.ndarray:
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        out = np.empty((self.P, self.P), dtype=np.float64)
+        rc = fn(self.solver, _dp(p), _dp(out), self.P)
+        if rc:
+            raise RuntimeError(f"quantum geometry verb: {rc}")
+        return out
+
+    def qgt(self, params) -> np.ndarray:
+        """moonlab_vqe_qgt: the metric g = Re Q."""
+        return self._tensor(self.lib.moonlab_vqe_qgt, params)
+
+    def berry_curvature(self, params) -> np.ndarray:
+        """moonlab_vqe_berry_curvature: F = -2 Im Q."""
+        return self._tensor(self.lib.moonlab_vqe_berry_curvature, params)
+
+    def natural_gradient_direction(self, params, gradient, regularization: float) -> np.ndarray:
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        gr = np.ascontiguousarray(gradient, dtype=np.float64)
+        out = np.empty(self.P, dtype=np.float64)
+        rc = self.lib.vqe_natural_gradient_direction(self.solver, _dp(p), _dp(gr), regularization, _dp(out))
+        if rc:
+            raise RuntimeError(f"vqe_natural_gradient_direction: {rc}")
+        return out
 
     def close(self):
         if self.solver:
