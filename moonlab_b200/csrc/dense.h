@@ -8,15 +8,20 @@
 // complex matrix per value of the conditioning qubits, in FP64, by applying
 // the ops in turn to the identity (row operations on all 16 columns at once)
 // with exactly the semantics of the register-group code (kernels_tile.cu:
-// op_pair, op_swap, op_diag and the tile predicates), and the real 32x32 form of each matrix is written in the
-// A-fragment order of mma.sync m8n8k4 f64 (row.col):
-//   fragment (i, s), lane l holds A[8 i + (l >> 2)][4 s + (l & 3)],
-//   real row 8 i + r  = component i & 1 (re, im) of output slot 8 (i >> 1) + r,
-//   real col 4 s + q  = component s & 1 of input slot 4 (s >> 1) + q,
-// (fragment slots are the register qubits in a chosen order, see below)
-// so a lane's B operands are the re and im parts of four whole input slots
-// and its D results the re and im parts of two whole output slots (one
-// 16-byte shared-memory access each).  Host-only.
+// op_pair, op_swap, op_diag and the tile predicates).  The kernel applies
+// U = R + iJ with three real products (Gauss's complex multiplication):
+//   t1 = R xr,  t2 = J xi,  t3 = (R + J)(xr + xi),
+//   yr = t1 - t2,  yi = t3 - t1 - t2,
+// 48 FP64 multiply-adds per amplitude instead of the 64 of the real 32x32
+// form.  R and J are written in the A-fragment order of mma.sync m8n8k4 f64
+// (row.col), R first:
+//   fragment (p, i, s), p = 0 (R) or 1 (J), i = 0..1, s = 0..3:
+//   lane l holds M[8 i + (l >> 2)][4 s + (l & 3)],
+//   row = output slot, column = input slot
+// (fragment slots are the register qubits in a chosen order, see below), so
+// a lane's B operands are four whole input slots (re, im) and its D results
+// two whole output slots (one 16-byte shared-memory access each); R + J is
+// formed in registers.  Host-only.
 #pragma once
 
 #include <cstring>
@@ -239,7 +244,8 @@ inline bool plan_segment(const DevPass& P, const DevSegment& sg, const DevOp* op
   return true;
 }
 
-// The matrices of a planned segment: S.nvar variants of 1024 doubles at out.
+// The matrices of a planned segment: S.nvar variants of kDenseVarDoubles
+// doubles at out.
 inline void fill_fragments(const DevSegment& sg, const DevOp* ops, const DenseSegDev& D, const SegPlan& S,
                            double* out) {
   // the ops before the first one that reads a conditioning bit are the same
@@ -282,15 +288,15 @@ inline void fill_fragments(const DevSegment& sg, const DevOp* ops, const DenseSe
     std::memcpy(Ur, Pr, sizeof Ur);
     std::memcpy(Ui, Pi, sizeof Ui);
     for (int o = first_dep; o < sg.op_end; o++) apply_rows(ops[o], locs, tb, Ur, Ui);
-    double* f = out + (size_t)v * 1024;
-    for (int i = 0; i < 4; i++)
-      for (int sk = 0; sk < 8; sk++)
-        for (int l = 0; l < 32; l++) {
-          const int ao = 8 * (i >> 1) + (l >> 2), co_ = i & 1;
-          const int ai = 4 * (sk >> 1) + (l & 3), ci = sk & 1;
-          const double ur = Ur[S.kappa[ao]][S.kappa[ai]], ui = Ui[S.kappa[ao]][S.kappa[ai]];
-          f[(i * 8 + sk) * 32 + l] = co_ == 0 ? (ci == 0 ? ur : -ui) : (ci == 0 ? ui : ur);
-        }
+    double* f = out + (size_t)v * kDenseVarDoubles;
+    for (int p = 0; p < 2; p++)
+      for (int i = 0; i < 2; i++)
+        for (int sk = 0; sk < 4; sk++)
+          for (int l = 0; l < 32; l++) {
+            const int ao = 8 * i + (l >> 2), ai = 4 * sk + (l & 3);
+            const double* row = p == 0 ? Ur[S.kappa[ao]] : Ui[S.kappa[ao]];
+            f[((p * 2 + i) * 4 + sk) * 32 + l] = row[S.kappa[ai]];
+          }
   }
 }
 
@@ -302,7 +308,7 @@ inline bool build_segment(const DevPass& P, const DevSegment& sg, const DevOp* o
   SegPlan S;
   if (!plan_segment(P, sg, ops, D, S)) return false;
   D.frag_off = (uint32_t)frags.size();
-  frags.resize(frags.size() + (size_t)S.nvar * 1024);
+  frags.resize(frags.size() + (size_t)S.nvar * kDenseVarDoubles);
   fill_fragments(sg, ops, D, S, frags.data() + D.frag_off);
   dsegs.push_back(D);
   return true;

@@ -569,7 +569,7 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
         dense::SegPlan S;
         if (dense::plan_segment(pp.pass, E->segs[si], E->dops.data(), D, S)) {
           D.frag_off = (uint32_t)nfrag;
-          nfrag += (size_t)S.nvar * 1024;
+          nfrag += (size_t)S.nvar * kDenseVarDoubles;
           dev_segs[si].mode = 2;
           dev_segs[si].dense = (int)dsegs.size();
           dsegs.push_back(D);

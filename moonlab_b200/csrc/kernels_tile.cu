@@ -22,14 +22,15 @@
 //
 // complex128 segments that the host multiplied into one 16x16 complex matrix
 // (dense.h; mode 2) run on the FP64 tensor cores instead: the tile's 512
-// groups of 16 amplitudes are the columns of a 32 x 512 real block, each warp
-// takes 8 groups at a time (an n = 8 column tile), loads them as the B
-// fragments of 8 k-steps (four 16-byte loads per lane), runs 4 m-tiles x 8
-// k-steps = 32 mma.sync m8n8k4 f64 with the matrix fragments in registers and
-// stores the D fragments back in place (four 16-byte stores per lane).  Gate
-// by gate, a segment's ~12 ops cost about as many FP64 multiply-adds as the
-// dense product (64 per amplitude) but spend two thirds of their instruction
-// issue on addressing, dispatch and register moves; one DMMA is 256 of them.
+// groups of 16 amplitudes are the columns of a 16 x 512 complex block, each
+// warp takes 8 groups at a time (an n = 8 column tile), loads them as the B
+// fragments of 4 k-steps (four 16-byte loads per lane), runs 3 real products
+// x 2 m-tiles x 4 k-steps = 24 mma.sync m8n8k4 f64 (Gauss's three-product
+// complex multiplication) with the matrix fragments in registers and stores
+// the results back in place (four 16-byte stores per lane).  Gate by gate, a
+// segment's ~12 ops cost about as many FP64 multiply-adds as the dense
+// product (48 per amplitude) but spend two thirds of their instruction issue
+// on addressing, dispatch and register moves; one DMMA is 256 of them.
 #include <atomic>
 #include <cstdio>
 
@@ -198,14 +199,31 @@ __device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, doubl
 }
 
 // Mode-2 segment: every group of the tile times the segment's dense matrix
-// (the variant of this group's and tile's conditioning bits).  Fragment
-// layout of mma.sync m8n8k4 f64 (lane l, r = l >> 2, c = l & 3): A[r][c],
-// B[c][r], D[r][2 c], D[r][2 c + 1]; the host stores the matrix so that
-// lane l's B operands are whole input slots 4 t + c of group r and its D
-// results whole output slots r and 8 + r of groups 2 c and 2 c + 1.
+// U = R + iJ (the variant of this group's and tile's conditioning bits), as
+// three real 16 x 16 products (Gauss): t1 = R xr, t2 = J xi,
+// t3 = (R + J)(xr + xi); yr = t1 - t2, yi = t3 - t1 - t2.  Fragment layout
+// of mma.sync m8n8k4 f64 (lane l, r = l >> 2, c = l & 3): A[r][c], B[c][r],
+// D[r][2 c], D[r][2 c + 1]; the host stores R and J so that lane l's B
+// operands are whole input slots 4 s + c of group r (re for t1, im for t2,
+// their sum for t3) and its D results whole output slots r and 8 + r of
+// groups 2 c and 2 c + 1.
+// Matrix variant of column tile j of a dense segment in the tile at tile_base.
+__device__ __forceinline__ int dense_variant(const DenseSegDev* __restrict__ sg, uint64_t tile_base, int j) {
+  const int nloc = sg->nloc, nout = sg->nout;
+  uint32_t vout = 0;
+  for (int k = 0; k < nout; k++) vout |= (uint32_t)((tile_base >> sg->obit[k]) & 1ull) << k;
+  return (nloc ? (j >> (6 - nloc)) : 0) | (int)(vout << nloc);
+}
+
+// pf: this warp's first matrix variant of the segment, loaded by the previous
+// dense segment (have_pf); nsg / nbase: the next dense segment and its tile,
+// whose first variant this call loads into pf during its last step, so the
+// L2 latency of the fragments overlaps that step and the barrier.
 template <int NT>
 __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const DenseSegDev* __restrict__ sg,
-                                              const double* __restrict__ frags, uint64_t tile_base) {
+                                              const double* __restrict__ frags, uint64_t tile_base,
+                                              bool have_pf, double (&pf)[16],
+                                              const DenseSegDev* __restrict__ nsg, uint64_t nbase) {
   constexpr int kWarps = NT / 32, kPerWarp = 64 / kWarps;  // 64 column tiles of 8 groups
   // warp w takes column tiles kPerWarp w .. + kPerWarp - 1: their conditioning
   // values (the top group-index bits) rarely change within a warp
@@ -220,8 +238,8 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
   const uint32_t glb = sg->g_lo[g8], gld0 = sg->g_lo[2 * q], gld1 = sg->g_lo[2 * q + 1];
   const double* fseg = frags + sg->frag_off + lane;
   int cur = -1;
-  double a[32];
-  // two column tiles per step: 8 independent accumulator chains per warp
+  double ar[8], aj[8], as[8];  // fragment (i, s) at index 4 i + s
+  // two column tiles per step: 12 independent accumulator chains per warp
   // cover the DMMA latency; they differ only in bit 0 of j, so they share
   // their conditioning values (the top nloc <= 5 of j's 6 bits)
 #pragma unroll 1
@@ -230,9 +248,22 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
     const uint32_t ghi0 = sg->g_hi[j], ghi1 = sg->g_hi[j + 1];
     const int var = (nloc ? (j >> (6 - nloc)) : 0) | (int)(vout << nloc);
     if (var != cur) {  // warp-uniform
-      const double* f = fseg + (size_t)var * 1024;
+      if (u == 0 && have_pf) {
 #pragma unroll
-      for (int k = 0; k < 32; k++) a[k] = __ldg(f + 32 * k);
+        for (int k = 0; k < 8; k++) {
+          ar[k] = pf[k];
+          aj[k] = pf[8 + k];
+        }
+      } else {
+        const double* f = fseg + (size_t)var * kDenseVarDoubles;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          ar[k] = __ldg(f + 32 * k);
+          aj[k] = __ldg(f + 32 * (8 + k));
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; k++) as[k] = ar[k] + aj[k];
       cur = var;
     }
     double2 x0[4], x1[4];
@@ -241,28 +272,47 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
       x0[t4] = sm[ghi0 ^ glb ^ boff[t4]];
       x1[t4] = sm[ghi1 ^ glb ^ boff[t4]];
     }
-    double d0[4][2], d1[4][2];
+    if (u == kPerWarp - 2 && nsg != nullptr) {  // last step: fetch the next segment's first variant
+      const double* f = frags + nsg->frag_off + lane +
+                        (size_t)dense_variant(nsg, nbase, kPerWarp * warp) * kDenseVarDoubles;
 #pragma unroll
-    for (int i = 0; i < 4; i++) d0[i][0] = d0[i][1] = d1[i][0] = d1[i][1] = 0.0;
+      for (int k = 0; k < 16; k++) pf[k] = __ldg(f + 32 * k);
+    }
+    // [column tile][product][m-tile][column]
+    double t[2][3][2][2];
 #pragma unroll
-    for (int sk = 0; sk < 8; sk++) {
-      const double b0 = (sk & 1) ? x0[sk >> 1].y : x0[sk >> 1].x;
-      const double b1 = (sk & 1) ? x1[sk >> 1].y : x1[sk >> 1].x;
+    for (int c = 0; c < 2; c++)
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        dmma_f64(d0[i][0], d0[i][1], a[i * 8 + sk], b0);
-        dmma_f64(d1[i][0], d1[i][1], a[i * 8 + sk], b1);
+      for (int p = 0; p < 3; p++)
+#pragma unroll
+        for (int i = 0; i < 2; i++) t[c][p][i][0] = t[c][p][i][1] = 0.0;
+#pragma unroll
+    for (int sk = 0; sk < 4; sk++) {
+      const double s0 = x0[sk].x + x0[sk].y, s1 = x1[sk].x + x1[sk].y;
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int f = 4 * i + sk;
+        dmma_f64(t[0][0][i][0], t[0][0][i][1], ar[f], x0[sk].x);
+        dmma_f64(t[1][0][i][0], t[1][0][i][1], ar[f], x1[sk].x);
+        dmma_f64(t[0][1][i][0], t[0][1][i][1], aj[f], x0[sk].y);
+        dmma_f64(t[1][1][i][0], t[1][1][i][1], aj[f], x1[sk].y);
+        dmma_f64(t[0][2][i][0], t[0][2][i][1], as[f], s0);
+        dmma_f64(t[1][2][i][0], t[1][2][i][1], as[f], s1);
       }
     }
     // in place: this warp's 16 groups are read above and by no other warp
-    sm[ghi0 ^ gld0 ^ doff0] = make_double2(d0[0][0], d0[1][0]);
-    sm[ghi0 ^ gld0 ^ doff1] = make_double2(d0[2][0], d0[3][0]);
-    sm[ghi0 ^ gld1 ^ doff0] = make_double2(d0[0][1], d0[1][1]);
-    sm[ghi0 ^ gld1 ^ doff1] = make_double2(d0[2][1], d0[3][1]);
-    sm[ghi1 ^ gld0 ^ doff0] = make_double2(d1[0][0], d1[1][0]);
-    sm[ghi1 ^ gld0 ^ doff1] = make_double2(d1[2][0], d1[3][0]);
-    sm[ghi1 ^ gld1 ^ doff0] = make_double2(d1[0][1], d1[1][1]);
-    sm[ghi1 ^ gld1 ^ doff1] = make_double2(d1[2][1], d1[3][1]);
+    auto out = [&](int c, int i, int col) {
+      const double t1 = t[c][0][i][col], t2 = t[c][1][i][col];
+      return make_double2(t1 - t2, t[c][2][i][col] - t1 - t2);
+    };
+    sm[ghi0 ^ gld0 ^ doff0] = out(0, 0, 0);
+    sm[ghi0 ^ gld0 ^ doff1] = out(0, 1, 0);
+    sm[ghi0 ^ gld1 ^ doff0] = out(0, 0, 1);
+    sm[ghi0 ^ gld1 ^ doff1] = out(0, 1, 1);
+    sm[ghi1 ^ gld0 ^ doff0] = out(1, 0, 0);
+    sm[ghi1 ^ gld0 ^ doff1] = out(1, 1, 0);
+    sm[ghi1 ^ gld1 ^ doff0] = out(1, 0, 1);
+    sm[ghi1 ^ gld1 ^ doff1] = out(1, 1, 1);
   }
 }
 
@@ -345,6 +395,8 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   const bool full = tile_amps == (1u << TB);
   const uint32_t sm_base = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
   bool prefetched = false;
+  double pf[16];  // next dense segment's first matrix variant (dense_segment)
+  bool have_pf = false;
   for (uint64_t tile = blockIdx.x; tile < pass.num_tiles; tile += gridDim.x) {
     const uint64_t tile_base = pdep64(tile, pass.tile_free_mask);
     // tile-constant op predicates and keys
@@ -383,10 +435,26 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
       const DevSegment& seg = ssegs[s];
       if constexpr (sizeof(Real) == 8) {
         if (seg.mode == 2) {
-          dense_segment<NT>(reinterpret_cast<double2*>(sm), dsegs + seg.dense, frags, tile_base);
+          // the next dense segment: this tile's next one, or the first of the
+          // CTA's next tile
+          const DenseSegDev* nsg = nullptr;
+          uint64_t nbase = tile_base;
+          if (s + 1 < nseg) {
+            if (ssegs[s + 1].mode == 2) nsg = dsegs + ssegs[s + 1].dense;
+          } else if (tile + gridDim.x < pass.num_tiles && ssegs[0].mode == 2) {
+            nsg = dsegs + ssegs[0].dense;
+            nbase = pdep64(tile + gridDim.x, pass.tile_free_mask);
+          }
+          dense_segment<NT>(reinterpret_cast<double2*>(sm), dsegs + seg.dense, frags, tile_base, have_pf, pf,
+                            nsg, nbase);
+          have_pf = nsg != nullptr;
           __syncthreads();
           continue;
         }
+        // pf is not carried across other segments (keeps it out of their registers)
+        have_pf = false;
+#pragma unroll
+        for (int k = 0; k < 16; k++) pf[k] = 0.0;
       }
       if (seg.mode == 1) {
         const int o = seg.op_begin;

@@ -75,7 +75,9 @@ struct DevPass {
 // ---- dense complex128 segments (dense.h, kernels_tile.cu) ----
 // A register segment of a complex128 tile pass applied as one 16x16 complex
 // matrix on its 4 register qubits, on the FP64 tensor cores (mma.sync m8n8k4
-// f64).  The matrix may depend on up to kDenseMaxCond conditioning qubits
+// f64) as three real 16x16 products (Gauss: Re U . Re x, Im U . Im x and
+// (Re U + Im U) . (Re x + Im x)).  The matrix may depend on up to
+// kDenseMaxCond conditioning qubits
 // outside the register set (controls or diagonal keys; tile-local ones vary
 // by group, outside ones by tile): one matrix variant per value of those
 // bits.  Offsets are in 16-byte tile elements, already swizzled (the tile
@@ -83,8 +85,10 @@ struct DevPass {
 constexpr int kDenseMaxCond = 6;     // conditioning qubits in all (64 variants)
 constexpr int kDenseMaxCondLoc = 5;  // of them tile-local (the top group-index bits; a column-tile pair shares one)
 constexpr int kDenseMaxCondOut = 6;  // of them outside the tile
+// doubles per matrix variant: Re U and Im U as 2 x 8 A fragments of 32 lanes
+constexpr int kDenseVarDoubles = 512;
 struct DenseSegDev {
-  uint32_t frag_off;   // first double of variant 0 in the fragment pool (1024 per variant)
+  uint32_t frag_off;   // first double of variant 0 in the fragment pool (kDenseVarDoubles per variant)
   uint8_t nloc;        // tile-local conditioning qubits: group-index bits 9 - nloc .. 8
   uint8_t nout;        // outside conditioning qubits: global bits obit[0 .. nout)
   uint8_t pad[2];
@@ -146,6 +150,14 @@ int launch_adj_pauli(int dtype, const void* psi, void* lam, const AdjPass& P, co
                      bool accumulate, bool energy, double* d_epart, int num_sms, cudaStream_t stream);
 int launch_adj_reduce(const double* d_partials, uint64_t tiles_per_state, int num_slots, uint64_t batch,
                       const int* d_param_of_slot, int num_params, double* d_out, cudaStream_t stream);
+
+// Gram matrix of B complex128 states stored back to back ([B][dim]):
+// d_G[a * B + b] = sum_x conj(S_a[x]) S_b[x] for a <= b (the rest of d_G is
+// not written), in FP64 with a fixed summation order (kernels_geometry.cu).
+// d_scratch: gram_scratch_bytes(B, dim, num_sms) bytes of device memory.
+size_t gram_scratch_bytes(int B, uint64_t dim, int num_sms);
+int launch_gram(const void* states, uint64_t dim, int B, double2* d_G, void* d_scratch, int num_sms,
+                cudaStream_t stream);
 
 // Kernel launchers (kernels_*.cu).  All asynchronous on `stream`.
 // d_dsegs / d_frags: the program's dense segments and their matrix fragments
