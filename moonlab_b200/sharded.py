@@ -19,8 +19,13 @@ and the layout records the swap.  The local qubit chosen is the one whose
 next use as a target is furthest ahead, so one swap serves many gates.
 
 The local ops run on an executor: `EngineExecutor` keeps the shard in an
-engine state on this rank's device (the tile kernels), and the exchange goes
-through torch.distributed (NCCL between devices).  `gather` returns the
+engine state on this rank's device (the tile kernels).  `ShardedState` runs
+one shard per rank and exchanges through torch.distributed (NCCL send/recv
+between devices); `LocalShards` holds all shards in one process and
+exchanges by device-to-device copies.  Either way an exchange moves the
+half-shard in chunks through one reusable staging buffer per direction, so
+it never needs more than one chunk of extra memory (the reference's bounded
+buffer_size exchange, distributed_gates.c:241-273).  `gather` returns the
 whole state in logical qubit order.
 """
 from __future__ import annotations
@@ -102,6 +107,9 @@ def plan(ops, n: int, g: int, lookahead: int = 512, start: Layout | None = None)
                 score = next_use(b, i + 1)
                 if score > best_score:
                     best, best_score = p, score
+            if best is None:
+                raise ValueError(f"op {i} has {len(tq)} targets but a shard has only {lay.n_loc} local "
+                                 "qubits: need more local qubits than the widest op has targets")
             j = lay.phys[q] - lay.n_loc
             steps.append(("swap", j, best))
             lay.swap(j, best)
@@ -168,23 +176,94 @@ def localize(o, phys, n_loc: int, rank: int):
     raise ValueError(f"op kind {o.kind} cannot be sharded")
 
 
-def exchange_half(shard, l: int, j: int, rank: int, group=None) -> None:
+DEFAULT_CHUNK = 1 << 24  # amplitudes per exchange chunk (256 MiB of complex128)
+
+
+def half_view(shard, l: int, j: int, rank: int):
+    """The half-shard that rank-bit j <-> local bit l moves off this rank: the
+    slots whose local bit l differs from this rank's bit j, as an R x C
+    strided view (C = 2^l contiguous amplitudes per row)."""
+    a = (rank >> j) & 1
+    n_half = shard.numel() // 2
+    return shard.view(n_half >> l, 2, 1 << l)[:, 1 - a, :]
+
+
+def chunks(rows: int, cols: int, chunk: int):
+    """Row-major blocks (r0, r1, c0, c1) of at most `chunk` elements that
+    cover a rows x cols view, the same sequence on every rank."""
+    if chunk < 1:
+        raise ValueError("chunk must be at least one amplitude")
+    if cols <= chunk:
+        step = max(1, chunk // cols)
+        for r0 in range(0, rows, step):
+            yield r0, min(rows, r0 + step), 0, cols
+    else:
+        for r in range(rows):
+            for c0 in range(0, cols, chunk):
+                yield r, r + 1, c0, min(cols, c0 + chunk)
+
+
+class Staging:
+    """The bounded staging an exchange goes through: one send and one receive
+    buffer of `chunk` amplitudes, allocated on first use and reused, so an
+    exchange never holds more than one chunk of extra memory per direction
+    (the reference exchanges through a fixed buffer_size in chunks,
+    distributed_gates.c:241-273)."""
+
+    def __init__(self, chunk: int = DEFAULT_CHUNK):
+        if chunk < 1:
+            raise ValueError("chunk must be at least one amplitude")
+        self.chunk = chunk
+        self.send = self.recv = None
+
+    def buffers(self, like):
+        k = min(self.chunk, like.numel() // 2)
+        if self.send is None or self.send.numel() < k or self.send.device != like.device:
+            self.send = like.new_empty(k)
+            self.recv = like.new_empty(k)
+        return self.send, self.recv
+
+
+def exchange_half(shard, l: int, j: int, rank: int, group=None, staging: Staging | None = None) -> None:
     """Rank-bit j <-> local bit l: swap the half-shard whose local bit l
     differs from this rank's bit j with the partner rank (rank ^ 2^j), slot
-    for slot, through a contiguous staging buffer."""
+    for slot, one staging chunk at a time (send and receive on the same
+    buffers for every chunk)."""
     import torch.distributed as dist
-    a = (rank >> j) & 1
+    staging = staging or Staging()
     partner = rank ^ (1 << j)
-    n_half = shard.numel() // 2
-    view = shard.view(n_half >> l, 2, 1 << l)[:, 1 - a, :]
-    send = view.contiguous()
-    recv = send.new_empty(send.shape)
     if group is not None:
         partner = dist.get_global_rank(group, partner)
-    ops = [dist.P2POp(dist.isend, send, partner, group), dist.P2POp(dist.irecv, recv, partner, group)]
-    for w in dist.batch_isend_irecv(ops):
-        w.wait()
-    view.copy_(recv)
+    view = half_view(shard, l, j, rank)
+    send, recv = staging.buffers(shard)
+    R, Cn = view.shape
+    for r0, r1, c0, c1 in chunks(R, Cn, send.numel()):
+        blk = view[r0:r1, c0:c1]
+        k = blk.numel()
+        s, r = send[:k].view(blk.shape), recv[:k].view(blk.shape)
+        s.copy_(blk)
+        ops = [dist.P2POp(dist.isend, send[:k], partner, group), dist.P2POp(dist.irecv, recv[:k], partner, group)]
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+        blk.copy_(r)
+
+
+def exchange_local(lo_shard, hi_shard, l: int, staging: Staging | None = None) -> None:
+    """The same exchange between two shards held by one process (rank r with
+    bit j = 0 and its partner r | 2^j, on one device or two): lo's half with
+    local bit l = 1 swaps with hi's half with bit l = 0, one staging chunk at
+    a time, as device-to-device copies."""
+    staging = staging or Staging()
+    va = half_view(lo_shard, l, 0, 0)
+    vb = half_view(hi_shard, l, 0, 1)
+    tmp, _ = staging.buffers(lo_shard)
+    R, Cn = va.shape
+    for r0, r1, c0, c1 in chunks(R, Cn, tmp.numel()):
+        a, b = va[r0:r1, c0:c1], vb[r0:r1, c0:c1]
+        t = tmp[:a.numel()].view(a.shape)
+        t.copy_(a)
+        a.copy_(b)
+        b.copy_(t)
 
 
 class EngineExecutor:
@@ -228,7 +307,7 @@ class ShardedState:
     """An n-qubit state over the ranks of `group` (a power of two), starting
     in |0...0>: rank 0's shard holds amplitude 0."""
 
-    def __init__(self, n: int, executor, group=None):
+    def __init__(self, n: int, executor, group=None, chunk: int = DEFAULT_CHUNK):
         import torch.distributed as dist
         self.ws = dist.get_world_size(group)
         self.rank = dist.get_rank(group)
@@ -240,6 +319,8 @@ class ShardedState:
         self.ex = executor
         self.layout = Layout(n, g)
         self.exchanges = 0
+        self.staging = Staging(chunk)
+        self.ex.sync()  # the executor's own initialisation has finished
         self.ex.shard.zero_()
         if self.rank == 0:
             self.ex.shard[0] = 1.0
@@ -257,7 +338,7 @@ class ShardedState:
             else:
                 _, j, l = st
                 self.ex.sync()
-                exchange_half(self.ex.shard, l, j, self.rank, self.group)
+                exchange_half(self.ex.shard, l, j, self.rank, self.group, self.staging)
                 self.ex.written()
                 self.layout.swap(j, l)
                 self.exchanges += 1
@@ -276,6 +357,68 @@ class ShardedState:
         parts = [torch.empty_like(loc) for _ in range(self.ws)]
         dist.all_gather(parts, loc, group=self.group)
         full = torch.cat([p.cpu() for p in parts]).numpy()  # physical index = rank << n_loc | local
+        n = self.n
+        src = [n - 1 - self.layout.phys[n - 1 - k] for k in range(n)]
+        return np.ascontiguousarray(full.reshape([2] * n).transpose(src)).reshape(-1)
+
+
+class LocalShards:
+    """An n-qubit state as 2^g shards held by one process: one executor per
+    shard, on one device or spread over this node's devices.  The same plan,
+    per-shard op rewrite and half-shard exchanges as ShardedState, with each
+    pair's exchange done as chunked device-to-device copies instead of
+    torch.distributed messages."""
+
+    def __init__(self, n: int, executors, chunk: int = DEFAULT_CHUNK):
+        W = len(executors)
+        g = W.bit_length() - 1
+        if W < 1 or 1 << g != W:
+            raise ValueError("the number of shards must be a power of two")
+        self.n, self.g, self.n_loc = n, g, n - g
+        self.ex = list(executors)
+        self.layout = Layout(n, g)
+        self.exchanges = 0
+        self.staging = Staging(chunk)
+        for r, e in enumerate(self.ex):
+            e.sync()
+            e.shard.zero_()
+            if r == 0:
+                e.shard[0] = 1.0
+            e.written()
+
+    def run_ops(self, ops) -> None:
+        """Apply engine ops (mlb_op_t records on logical qubits) in order."""
+        ops = list(ops)
+        steps, _ = plan(ops, self.n, self.g, start=self.layout)
+        for st in steps:
+            if st[0] == "ops":
+                _, phys, idx = st
+                for r, e in enumerate(self.ex):
+                    local = [localize(ops[i], phys, self.n_loc, r) for i in idx]
+                    e.apply([o for o in local if o is not None])
+            else:
+                _, j, l = st
+                for e in self.ex:
+                    e.sync()
+                for r in range(len(self.ex)):
+                    if not (r >> j) & 1:
+                        exchange_local(self.ex[r].shard, self.ex[r | (1 << j)].shard, l, self.staging)
+                for e in self.ex:
+                    e.written()
+                self.layout.swap(j, l)
+                self.exchanges += 1
+        for e in self.ex:
+            e.sync()
+
+    def run(self, gates) -> None:
+        """Apply gate records (the QGTL enum and its extensions)."""
+        from .statevector import gates_to_ops
+        self.run_ops(gates_to_ops(gates, self.n))
+
+    def gather(self):
+        """The whole state in logical qubit order (numpy)."""
+        import torch
+        full = torch.cat([e.shard.detach().cpu() for e in self.ex]).numpy()
         n = self.n
         src = [n - 1 - self.layout.phys[n - 1 - k] for k in range(n)]
         return np.ascontiguousarray(full.reshape([2] * n).transpose(src)).reshape(-1)

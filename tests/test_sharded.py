@@ -139,7 +139,40 @@ class NumpyExecutor:
         pass
 
 
-def _rank(rank, ws, port, n, name, q):
+@pytest.mark.parametrize("rows,cols,chunk", [(1, 1, 1), (8, 4, 5), (8, 4, 4), (3, 16, 5), (2, 64, 64), (5, 1, 3)])
+def test_chunks_cover_the_view_once(rows, cols, chunk):
+    seen = np.zeros((rows, cols), int)
+    for r0, r1, c0, c1 in S.chunks(rows, cols, chunk):
+        assert (r1 - r0) * (c1 - c0) <= chunk
+        seen[r0:r1, c0:c1] += 1
+    assert (seen == 1).all()
+
+
+def test_planner_rejects_too_few_local_qubits():
+    # one local qubit cannot host a SWAP whose other target is a rank bit
+    n, g = 2, 1
+    ops = list(gates_to_ops(np.array([(13, 1, 0, 0, 0.0)], dtype=GATE_DTYPE), n))
+    with pytest.raises(ValueError, match="local qubits"):
+        S.plan(ops, n, g)
+
+
+@pytest.mark.parametrize("g,chunk", [(1, 3), (2, 16), (3, 1 << 20)])
+@pytest.mark.parametrize("name", list(CIRCUITS))
+def test_local_shards_match_the_whole_state(name, g, chunk):
+    # all shards in one process, exchanged in chunks of `chunk` amplitudes
+    n = 9
+    gates = CIRCUITS[name](n)
+    st = S.LocalShards(n, [NumpyExecutor(n - g) for _ in range(1 << g)], chunk=chunk)
+    half = len(gates) // 2
+    st.run(gates[:half])
+    st.run(gates[half:])
+    want = whole_state(n, list(gates_to_ops(gates, n)))
+    assert np.abs(st.gather() - want).max() < TOL
+    assert st.exchanges > 0
+    assert st.staging.send.numel() == min(chunk, 1 << (n - g - 1))  # the only extra memory
+
+
+def _rank(rank, ws, port, n, name, q, chunk=S.DEFAULT_CHUNK):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(ws))
     sys.path.insert(0, str(ROOT))
     sys.path.insert(0, str(ROOT / "tests"))
@@ -148,7 +181,7 @@ def _rank(rank, ws, port, n, name, q):
     dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
     try:
         g = ws.bit_length() - 1
-        st = S.ShardedState(n, NumpyExecutor(n - g))
+        st = S.ShardedState(n, NumpyExecutor(n - g), chunk=chunk)
         gates = CIRCUITS[name](n)
         half = len(gates) // 2
         st.run(gates[:half])  # two calls: the second starts from a permuted layout
@@ -159,14 +192,15 @@ def _rank(rank, ws, port, n, name, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("ws,name", [(2, "brickwork"), (2, "random"), (4, "qaoa"), (4, "random")])
-def test_gloo_ranks_match_the_whole_state(ws, name):
+@pytest.mark.parametrize("ws,name,chunk", [(2, "brickwork", S.DEFAULT_CHUNK), (2, "random", 7),
+                                           (4, "qaoa", 32), (4, "random", S.DEFAULT_CHUNK)])
+def test_gloo_ranks_match_the_whole_state(ws, name, chunk):
     import torch.multiprocessing as mp
     n = 9
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, ws, port, n, name, q)) for r in range(ws)]
+    procs = [ctx.Process(target=_rank, args=(r, ws, port, n, name, q, chunk)) for r in range(ws)]
     for p in procs:
         p.start()
     res = [q.get(timeout=240) for _ in range(ws)]
