@@ -480,6 +480,17 @@ int  mlb_hea_set_checkpointing(mlb_hea_t *h, int mode);
  * checkpoints, and how many sub-batches it ran. */
 int  mlb_hea_last_eval_stats(const mlb_hea_t *h, uint32_t *segment_layers, int *checkpoints_used,
                              size_t *sub_batches);
+/* Quantum geometry at one parameter vector (complex128 problems): the
+ * Fubini-Study metric g = Re Q and the Berry curvature F = -2 Im Q of
+ * Q_ij = <d_i psi|d_j psi> - <d_i psi|psi><psi|d_j psi>, each P x P
+ * row-major (either may be NULL), filled as vqe_compute_qgt and
+ * vqe_compute_berry_curvature fill them (src/algorithms/vqe_qng.c:166-232;
+ * replaces the per-entry host loops behind moonlab_vqe_qgt /
+ * moonlab_vqe_berry_curvature, src/applications/moonlab_vqe_export.c:53-86).
+ * psi and the P derivative states run as one batch of P + 1 states through
+ * the forward passes, and their Gram matrix comes from one FP64 kernel:
+ * (P + 1) states of 2^N amplitudes must fit on the device. */
+int  mlb_hea_geometry(mlb_hea_t *h, const double *params, double *metric, double *curvature);
 const char *mlb_hea_last_error(void);
 
 /* ---- error text ---------------------------------------------------------- */

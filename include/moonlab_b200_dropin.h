@@ -100,14 +100,94 @@ int moonlab_cuda_select_device_for_rank(int local_rank, int *device_id, int *dev
  *      src/applications/moonlab_vqe_export.c:27-42).  solver is the
  *      reference's vqe_solver_t (src/algorithms/vqe.h:545-568).  Returns 0 ok,
  *      -1 NULL argument, -2 num_parameters != ansatz->num_parameters, -3
- *      failure: noise model enabled (no exact gradient, as the reference's
- *      exact-or-error contract), an ansatz other than the hardware-efficient
- *      one, or a device error.  The batched variant takes params[B][P] and
- *      writes grads[B][P] with the same codes. ---- */
+ *      failure.  Hardware-efficient ansatz, no noise: the batched adjoint
+ *      engine.  UCCSD or symmetry-preserving ansatz, no noise: the
+ *      reference's exact four-term parameter-shift rule (vqe.c:2072-2140),
+ *      the shifted energies on the device.  A noise model without the
+ *      solver's allow_stochastic_gradient: -3 (exact-or-error, vqe.c:2060-2066).
+ *      A CUSTOM ansatz, or a noisy solver that opted into stochastic
+ *      parameter shift: the reference's own vqe_compute_gradient, found at
+ *      run time in the process (-3 when absent).  The batched variant takes
+ *      params[B][P] and writes grads[B][P] with the same codes. ---- */
 int moonlab_vqe_gradient(void *solver, const double *parameters, double *gradient_out,
                          size_t num_parameters);
 int moonlab_b200_vqe_gradient_batch(void *solver, size_t batch, const double *parameters,
                                     double *gradients_out, size_t num_parameters);
+
+/* ---- Quantum geometry verbs (src/applications/moonlab_vqe_export.c:53-100,
+ *      ABI 0.7.0).  Same codes as moonlab_vqe_gradient.  qgt_out / berry_out:
+ *      num_parameters^2 doubles, row-major, filled as vqe_compute_qgt and
+ *      vqe_compute_berry_curvature fill them (src/algorithms/vqe_qng.c:166-232);
+ *      direction_out = (g + regularization I)^-1 gradient by the same
+ *      partial-pivot elimination (vqe_qng.c:236-282; a pivot below 1e-300 is
+ *      singular: -3, and the caller falls back to the plain gradient as with
+ *      the reference).  Hardware-efficient ansatz: psi and the P derivative
+ *      states as one device batch and an FP64 Gram kernel (mlb_hea_geometry).
+ *      Other ansaetze: the reference's own vqe_compute_qgt /
+ *      vqe_compute_berry_curvature / vqe_natural_gradient_direction, found at
+ *      run time in the process (-3 when absent). ---- */
+int moonlab_vqe_qgt(void *solver, const double *parameters, double *qgt_out, size_t num_parameters);
+int moonlab_vqe_berry_curvature(void *solver, const double *parameters, double *berry_out,
+                                size_t num_parameters);
+int moonlab_vqe_natural_gradient(void *solver, const double *parameters, const double *gradient,
+                                 double regularization, double *direction_out, size_t num_parameters);
+
+/* ---- single-qubit gate fusion (src/optimization/fusion/fusion.h:73-458,
+ *      definitions src/optimization/fusion/fusion.c:127-394).
+ *      Same records, validation (-1 on a bad qubit or a == b) and run-length
+ *      rule in fuse_compile (FUSED_1Q products, fusion.c:247-292).
+ *      fuse_execute queues the whole list on the engine in one call: on a
+ *      GPU-backed state its own device state; on a host state a temporary
+ *      device state (uploaded, run, read back).  QS_ERROR_INVALID_STATE on
+ *      NULL arguments, QS_ERROR_INVALID_DIMENSION when the state has fewer
+ *      qubits than the circuit, as the reference. ---- */
+#ifndef MOONLAB_B200_USE_REFERENCE_TYPES
+typedef enum {
+    FUSE_GATE_H = 0, FUSE_GATE_X, FUSE_GATE_Y, FUSE_GATE_Z, FUSE_GATE_S, FUSE_GATE_SDG,
+    FUSE_GATE_T, FUSE_GATE_TDG, FUSE_GATE_PHASE, FUSE_GATE_RX, FUSE_GATE_RY, FUSE_GATE_RZ,
+    FUSE_GATE_U3, FUSE_GATE_FUSED_1Q, FUSE_GATE_CNOT, FUSE_GATE_CZ, FUSE_GATE_CY, FUSE_GATE_SWAP,
+    FUSE_GATE_CPHASE, FUSE_GATE_CRX, FUSE_GATE_CRY, FUSE_GATE_CRZ
+} fuse_gate_kind_t;
+typedef struct {            /* fusion.h:99-104; u is complex_t u[2][2] in C */
+    int    kind;
+    int    q[2];
+    double p[3];
+    double u[2][2][2];
+} fuse_gate_t;
+typedef struct fuse_circuit_t fuse_circuit_t;
+typedef struct {
+    size_t original_gates;
+    size_t fused_gates;
+    size_t merges_applied;
+} fuse_stats_t;
+#endif
+fuse_circuit_t *fuse_circuit_create(size_t num_qubits);
+void   fuse_circuit_free(fuse_circuit_t *c);
+size_t fuse_circuit_len(const fuse_circuit_t *c);
+size_t fuse_circuit_num_qubits(const fuse_circuit_t *c);
+int fuse_append_h(fuse_circuit_t *c, int q);
+int fuse_append_x(fuse_circuit_t *c, int q);
+int fuse_append_y(fuse_circuit_t *c, int q);
+int fuse_append_z(fuse_circuit_t *c, int q);
+int fuse_append_s(fuse_circuit_t *c, int q);
+int fuse_append_sdg(fuse_circuit_t *c, int q);
+int fuse_append_t(fuse_circuit_t *c, int q);
+int fuse_append_tdg(fuse_circuit_t *c, int q);
+int fuse_append_phase(fuse_circuit_t *c, int q, double theta);
+int fuse_append_rx(fuse_circuit_t *c, int q, double theta);
+int fuse_append_ry(fuse_circuit_t *c, int q, double theta);
+int fuse_append_rz(fuse_circuit_t *c, int q, double theta);
+int fuse_append_u3(fuse_circuit_t *c, int q, double theta, double phi, double lambda);
+int fuse_append_cnot(fuse_circuit_t *c, int ctrl, int tgt);
+int fuse_append_cz(fuse_circuit_t *c, int ctrl, int tgt);
+int fuse_append_cy(fuse_circuit_t *c, int ctrl, int tgt);
+int fuse_append_swap(fuse_circuit_t *c, int a, int b);
+int fuse_append_cphase(fuse_circuit_t *c, int ctrl, int tgt, double theta);
+int fuse_append_crx(fuse_circuit_t *c, int ctrl, int tgt, double theta);
+int fuse_append_cry(fuse_circuit_t *c, int ctrl, int tgt, double theta);
+int fuse_append_crz(fuse_circuit_t *c, int ctrl, int tgt, double theta);
+fuse_circuit_t *fuse_compile(const fuse_circuit_t *src, fuse_stats_t *stats);
+qs_error_t fuse_execute(const fuse_circuit_t *c, quantum_state_t *state);
 
 /* ---- scheduler backend plug-in (src/distributed/scheduler.h:225-262,
  *      registry scheduler.c:283-305).

@@ -160,6 +160,12 @@ _SIGS = {
     "mlb_hea_last_eval_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_int),
                                           C.POINTER(C.c_size_t)]),
     "moonlab_vqe_gradient": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_size_t]),
+    "mlb_hea_geometry": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "moonlab_vqe_qgt": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_size_t]),
+    "moonlab_vqe_berry_curvature": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                              C.c_size_t]),
+    "moonlab_vqe_natural_gradient": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                               C.c_double, C.POINTER(C.c_double), C.c_size_t]),
     "moonlab_b200_vqe_gradient_batch": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), C.c_size_t]),
     "mlb_job_parse_json": (C.c_int, [C.c_char_p, C.c_void_p, C.c_void_p, C.c_size_t,

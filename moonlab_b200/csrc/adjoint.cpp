@@ -103,6 +103,8 @@ struct mlb_hea {
   int* d_slots = nullptr;
   double* d_out = nullptr;  // [B] energies then [B][P] grads
   size_t out_cap = 0;
+  unsigned char* d_gram = nullptr;  // geometry: Gram matrix, then the Gram kernel's scratch
+  size_t gram_cap = 0;
   size_t budget = 0;         // bytes for psi + lambda; 0 = 80% of free memory
 };
 
@@ -447,9 +449,102 @@ int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, do
   return MLB_OK;
 }
 
+// The quantum geometric tensor of the ansatz at one parameter vector.
+// A rotation R(t) = exp(-i t G / 2) (G = Y for RY, Z for RZ) satisfies
+// G R(t) = i R(t + pi), so the reference's derivative state
+// d_i psi = (-i/2) U_after G_i U_upto |hf> (vqe_qng.c:60-99) equals
+// (1/2) psi(theta + pi e_i): the ansatz with parameter i's cos/sin pair
+// (c, s) replaced by (-s, c), exactly.  psi and the P shifted states run as
+// one batch of P + 1 vectors through the forward passes, and the Gram
+// matrix of the batch gives every inner product:
+//   <psi|d_i psi> = G[0][i+1] / 2,  <d_i psi|d_j psi> = G[i+1][j+1] / 4.
+// Q_ij = <d_i psi|d_j psi> - conj(<psi|d_i psi>) <psi|d_j psi>; the metric
+// and the curvature are filled as vqe_compute_qgt (vqe_qng.c:166-196) and
+// vqe_compute_berry_curvature (:198-232) fill them.
+int geometry(mlb_hea* h, const double* params, double* metric, double* curvature) {
+  if (h->dtype != MLB_C128) return hfail(MLB_ERR_NOT_SUPPORTED, "geometry needs a complex128 problem");
+  const size_t P = h->P, B = P + 1;
+  const size_t dim = (size_t)1 << h->n;
+  int rc;
+  std::vector<double2> cs(B * P);
+  for (size_t p = 0; p < P; p++) cs[p] = make_double2(std::cos(params[p] / 2.0), std::sin(params[p] / 2.0));
+  for (size_t i = 0; i < P; i++) {
+    std::memcpy(&cs[(i + 1) * P], cs.data(), P * sizeof(double2));
+    cs[(i + 1) * P + i] = make_double2(-cs[i].y, cs[i].x);
+  }
+  if ((rc = grow(h->d_cs, h->cs_cap, cs.size()))) return rc;
+  cudaMemcpyAsync(h->d_cs, cs.data(), cs.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream);
+  if (h->batch_cap < B) {
+    if (h->psi) cudaFree(h->psi);
+    if (h->lamb) cudaFree(h->lamb);
+    h->psi = h->lamb = nullptr;
+    h->batch_cap = 0;
+    cudaError_t e = cudaMalloc(&h->psi, B * dim * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&h->lamb, B * dim * 16);
+    if (e != cudaSuccess) return cfail(e, "geometry: P + 1 states");
+    h->batch_cap = B;
+  }
+  const size_t gbytes = B * B * sizeof(double2);
+  const size_t need = gbytes + gram_scratch_bytes((int)B, dim, h->num_sms);
+  size_t cap = h->gram_cap;
+  if ((rc = grow(h->d_gram, cap, (need + 255) / 256 * 256))) return rc;
+  h->gram_cap = cap;
+  if ((rc = launch_adj_init(h->dtype, h->psi, (int)h->n, B, 0, h->stream))) return hfail(rc, "init kernel");
+  for (const GatePass& gp : h->fwd) {
+    AdjPass Pp = gp.P;
+    Pp.num_tiles = Pp.tiles_per_state * B;
+    if ((rc = launch_adj_gates(h->dtype, h->psi, nullptr, Pp, h->d_ops + gp.ops_off, h->d_cs, nullptr, false,
+                               false, h->num_sms, h->stream)))
+      return hfail(rc, "forward pass");
+  }
+  double2* d_G = reinterpret_cast<double2*>(h->d_gram);
+  if ((rc = launch_gram(h->psi, dim, (int)B, d_G, h->d_gram + (gbytes + 255) / 256 * 256, h->num_sms, h->stream)))
+    return hfail(rc, "Gram kernel");
+  std::vector<double2> G(B * B);
+  cudaMemcpyAsync(G.data(), d_G, gbytes, cudaMemcpyDeviceToHost, h->stream);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return cfail(e, "geometry");
+  // a register padded to 3 qubits (n < 3) carries the idle qubits in |0>:
+  // the inner products are those of the n-qubit problem
+  std::vector<double> ovr(P), ovi(P);
+  for (size_t i = 0; i < P; i++) {
+    ovr[i] = G[i + 1].x * 0.5;  // row 0: <psi|psi_{i+1}>
+    ovi[i] = G[i + 1].y * 0.5;
+  }
+  for (size_t i = 0; i < P; i++)
+    for (size_t j = i; j < P; j++) {
+      const double2 g = G[(i + 1) * B + (j + 1)];
+      const double ar = g.x * 0.25, ai = g.y * 0.25;
+      // conj(ov_i) * ov_j
+      const double cr = ovr[i] * ovr[j] + ovi[i] * ovi[j];
+      const double ci = ovr[i] * ovi[j] - ovi[i] * ovr[j];
+      if (metric) {
+        const double v = ar - cr;
+        metric[i * P + j] = v;
+        metric[j * P + i] = v;
+      }
+      if (curvature) {
+        if (i == j) {
+          curvature[i * P + i] = 0.0;
+        } else {
+          const double F = -2.0 * (ai - ci);
+          curvature[i * P + j] = F;
+          curvature[j * P + i] = -F;
+        }
+      }
+    }
+  return MLB_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int mlb_hea_geometry(mlb_hea_t* h, const double* params, double* metric, double* curvature) {
+  if (!h || !params) return hfail(MLB_ERR_INVALID_ARG, "null argument");
+  Guard g(h->device);
+  return geometry(h, params, metric, curvature);
+}
 
 int mlb_hea_create(uint32_t n, uint32_t layers, uint64_t hf, size_t num_terms, const uint64_t* xm,
                    const uint64_t* zm, const double* coeffs, int dtype, int device, mlb_hea_t** out) {
@@ -535,7 +630,7 @@ void mlb_hea_free(mlb_hea_t* h) {
   Guard g(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (void* p : {h->psi, h->lamb, h->ckpt, (void*)h->d_cs, (void*)h->d_part, (void*)h->d_epart,
-                  (void*)h->d_ops, (void*)h->d_terms, (void*)h->d_slots, (void*)h->d_out})
+                  (void*)h->d_ops, (void*)h->d_terms, (void*)h->d_slots, (void*)h->d_out, (void*)h->d_gram})
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;

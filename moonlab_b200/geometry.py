@@ -3,22 +3,23 @@ tensor Q_ij = <d_i psi|d_j psi> - <d_i psi|psi><psi|d_j psi>, its real part
 (the Fubini-Study metric of quantum natural gradient) and its curvature part
 F = -2 Im Q, and the natural-gradient direction (g + lambda I)^-1 grad.
 
-Reference: src/algorithms/vqe_qng.c:42-58 (the trial state from the
-Hartree-Fock bits), :60-99 (exact derivatives by generator insertion: the
-Pauli generator right after the parameter's rotation, times -i/2),
-:101-164 (psi, the derivatives and <psi|d_i psi>), :166-196
-(vqe_compute_qgt), :198-232 (vqe_compute_berry_curvature), :270-282
-(vqe_natural_gradient_direction); src/applications/moonlab_vqe_export.c:53-90
-(moonlab_vqe_qgt, moonlab_vqe_berry_curvature).  The ansatz is
-vqe_apply_hardware_efficient_ansatz: per layer RY(q, theta_p) and
-RZ(q, theta_p+1) on every qubit, then CNOT(q, q+1) down the register.
+Reference: src/algorithms/vqe_qng.c:60-99 (exact derivatives by generator
+insertion: the Pauli generator right after the parameter's rotation, times
+-i/2), :166-196 (vqe_compute_qgt), :198-232 (vqe_compute_berry_curvature),
+:236-282 (spd_solve, vqe_natural_gradient_direction);
+src/applications/moonlab_vqe_export.c:53-100 (the stable verbs).
 
-The P derivative states are P circuit runs of the engine on the device, kept
-as the rows of one P x 2^n device matrix, and Q comes from one Hermitian
-Gram product of that matrix (a library GEMM) -- where the reference forms
-every entry with its own loop over 2^n amplitudes on the host.
+A rotation R(t) = exp(-i t G / 2) satisfies G R(t) = i R(t + pi), so the
+reference's derivative state d_i psi = (-i/2) U_after G_i U_upto |hf> is
+(1/2) psi(theta + pi e_i).  The engine runs psi and the P shifted states as
+one batch of P + 1 parameter vectors through the adjoint's forward passes
+and forms every inner product with one FP64 Gram kernel (mlb_hea_geometry),
+where the reference replays P circuits and loops over 2^n amplitudes per
+tensor entry on the host.
 """
 from __future__ import annotations
+
+import math
 
 import numpy as np
 
@@ -50,80 +51,62 @@ def hea_gates(n: int, layers: int, params, hf_reference: int = 0, insert: int | 
     return np.array(recs, dtype=GATE_DTYPE)
 
 
-class EngineRunner:
-    """Runs gate records on one complex128 engine state on `device` and
-    returns the output state as a device tensor (a copy)."""
-
-    def __init__(self, n: int, device: int = 0):
-        import torch
-        from .statevector import StateVector
-        self.sv = StateVector(n, "c128", device=device)
-        self.view = torch.as_tensor(_DeviceView(self.sv.device_ptr(), 1 << n), device=f"cuda:{device}")
-
-    def __call__(self, gates):
-        self.sv.reset()
-        self.sv.run(gates)
-        self.sv.synchronize()
-        return self.view.clone()
-
-    def close(self) -> None:
-        self.sv.close()
+def shifted_parameters(params) -> np.ndarray:
+    """The batch the engine runs: row 0 = theta, row i + 1 = theta + pi e_i
+    (d_i psi = psi(row i + 1) / 2)."""
+    th = np.asarray(params, dtype=np.float64).reshape(-1)
+    B = np.repeat(th[None, :], th.size + 1, axis=0)
+    B[1 + np.arange(th.size), np.arange(th.size)] += math.pi
+    return B
 
 
-class _DeviceView:
-    def __init__(self, ptr, count):
-        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<c16", "data": (ptr, False),
-                                         "version": 3, "strides": None}
+def geometry(n: int, layers: int, params, hf_reference: int = 0, device: int = 0):
+    """(metric, curvature), each P x P, on the device (complex128)."""
+    from .vqe import HEAProblem
+    prob = HEAProblem(n, layers, [], xmasks=[], zmasks=[], hf_reference=hf_reference, device=device)
+    try:
+        return prob.geometry(params)
+    finally:
+        prob.close()
 
 
-def state_and_derivatives(n: int, layers: int, params, run, hf_reference: int = 0):
-    """psi (2^n), D (P x 2^n, row i = d_i psi = -i/2 U_after P_i U_upto |HF>)
-    and ov (P, <psi|d_i psi>) as tensors on the runner's device."""
-    import torch
-    P = 2 * n * layers
-    psi = run(hea_gates(n, layers, params, hf_reference))
-    D = torch.empty((P, psi.numel()), dtype=torch.complex128, device=psi.device)
-    for i in range(P):
-        D[i] = run(hea_gates(n, layers, params, hf_reference, insert=i))
-    D *= -0.5j
-    ov = D @ psi.conj()  # <psi|d_i psi>
-    return psi, D, ov
-
-
-def geometric_tensor(n: int, layers: int, params, run, hf_reference: int = 0):
-    """Q (P x P complex, Hermitian up to rounding) as a device tensor."""
-    _, D, ov = state_and_derivatives(n, layers, params, run, hf_reference)
-    A = D.conj() @ D.T  # <d_i psi|d_j psi>
-    return A - torch_outer(ov.conj(), ov)
-
-
-def torch_outer(a, b):
-    return a[:, None] * b[None, :]
-
-
-def _mirror_upper(M, antisymmetric: bool):
-    """Upper triangle kept, lower filled from it, as the reference fills both
-    halves from one computed entry (exact (anti)symmetry)."""
-    import torch
-    up = torch.triu(M, diagonal=0 if not antisymmetric else 1)
-    return up - up.T if antisymmetric else up + torch.triu(M, diagonal=1).T
-
-
-def metric(n: int, layers: int, params, run, hf_reference: int = 0) -> np.ndarray:
+def metric(n: int, layers: int, params, hf_reference: int = 0, device: int = 0) -> np.ndarray:
     """g = Re Q (vqe_compute_qgt), P x P, symmetric."""
-    Q = geometric_tensor(n, layers, params, run, hf_reference)
-    return _mirror_upper(Q.real, False).cpu().numpy()
+    return geometry(n, layers, params, hf_reference, device)[0]
 
 
-def berry_curvature(n: int, layers: int, params, run, hf_reference: int = 0) -> np.ndarray:
+def berry_curvature(n: int, layers: int, params, hf_reference: int = 0, device: int = 0) -> np.ndarray:
     """F = -2 Im Q (vqe_compute_berry_curvature), P x P, antisymmetric."""
-    Q = geometric_tensor(n, layers, params, run, hf_reference)
-    return _mirror_upper(-2.0 * Q.imag, True).cpu().numpy()
+    return geometry(n, layers, params, hf_reference, device)[1]
 
 
-def natural_gradient_direction(g: np.ndarray, gradient, regularization: float) -> np.ndarray:
-    """(g + regularization I)^-1 gradient (vqe_natural_gradient_direction):
-    a P x P solve with partial pivoting; a singular system raises."""
+def natural_gradient_direction(g: np.ndarray, gradient, regularization: float):
+    """(g + regularization I)^-1 gradient by the reference's Gaussian
+    elimination with partial pivoting (spd_solve, vqe_qng.c:236-266).  A
+    pivot below 1e-300 makes the system singular: returns None, where the
+    reference returns -1 and its caller falls back to the plain gradient."""
     A = np.array(g, dtype=np.float64, copy=True)
-    A[np.diag_indices_from(A)] += regularization
-    return np.linalg.solve(A, np.asarray(gradient, dtype=np.float64))
+    n = A.shape[0]
+    A[np.diag_indices(n)] += regularization
+    w = np.array(gradient, dtype=np.float64, copy=True)
+    for col in range(n):
+        piv = col + int(np.argmax(np.abs(A[col:, col])))
+        if abs(A[piv, col]) < 1e-300:
+            return None
+        if piv != col:
+            A[[col, piv]] = A[[piv, col]]
+            w[[col, piv]] = w[[piv, col]]
+        d = A[col, col]
+        for r in range(col + 1, n):
+            f = A[r, col] / d
+            if f == 0.0:
+                continue
+            A[r, col:] -= f * A[col, col:]
+            w[r] -= f * w[col]
+    x = np.zeros(n)
+    for i in range(n - 1, -1, -1):
+        s = w[i]
+        for c in range(i + 1, n):
+            s -= A[i, c] * x[c]
+        x[i] = s / A[i, i]
+    return x

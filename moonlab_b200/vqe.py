@@ -102,6 +102,22 @@ class HEAProblem:
             raise MlbError(rc, "mlb_hea_evaluate", self._lib.mlb_hea_last_error().decode())
         return E, G
 
+    def geometry(self, params):
+        """(metric g = Re Q, curvature F = -2 Im Q), each P x P, of the
+        quantum geometric tensor at one parameter vector (complex128
+        problems): psi and the P derivative states as one device batch and
+        an FP64 Gram kernel (mlb_hea_geometry)."""
+        p = np.ascontiguousarray(params, dtype=np.float64).reshape(-1)
+        if p.size != self.num_parameters:
+            raise ValueError(f"expected {self.num_parameters} parameters")
+        P = self.num_parameters
+        g = np.empty((P, P), dtype=np.float64)
+        f = np.empty((P, P), dtype=np.float64)
+        rc = self._lib.mlb_hea_geometry(self._h, p.ctypes.data, g.ctypes.data, f.ctypes.data)
+        if rc:
+            raise MlbError(rc, "mlb_hea_geometry", self._lib.mlb_hea_last_error().decode())
+        return g, f
+
     def evaluate_torch(self, params, want_grad: bool = True):
         """params: torch float64 tensor [B, P] on cuda -> (E, G) cuda tensors."""
         import torch

@@ -191,7 +191,10 @@ def ref():
     """The reference's library (liboracle.so) with the signatures tests use."""
     global _ref
     if _ref is None:
-        lib = C.CDLL(str(REF_LIB), mode=os.RTLD_LOCAL)
+        # RTLD_DEEPBIND: the reference resolves its own symbols first, so the
+        # drop-in's definitions of the same names (loaded globally, e.g.
+        # fuse_circuit_create) never stand in for the reference's internals
+        lib = C.CDLL(str(REF_LIB), mode=os.RTLD_LOCAL | os.RTLD_DEEPBIND)
         sp = C.POINTER(RefState)
         i, d, u64, sz = C.c_int, C.c_double, C.c_uint64, C.c_size_t
         sigs = {
@@ -229,9 +232,17 @@ def ref():
             "moonlab_job_to_json": (i, [C.c_void_p, C.c_char_p, sz]),
             "moonlab_scheduler_run": (i, [C.c_void_p, C.POINTER(JobResults)]),
             "moonlab_job_results_free": (None, [C.POINTER(JobResults)]),
+            "fuse_circuit_create": (C.c_void_p, [sz]), "fuse_circuit_free": (None, [C.c_void_p]),
+            "fuse_circuit_len": (sz, [C.c_void_p]), "fuse_compile": (C.c_void_p, [C.c_void_p, C.c_void_p]),
+            "fuse_execute": (i, [C.c_void_p, sp]),
+            "fuse_append_u3": (i, [C.c_void_p, i, d, d, d]),
             "pauli_hamiltonian_create": (C.c_void_p, [sz, sz]),
             "pauli_hamiltonian_add_term": (i, [C.c_void_p, d, C.c_char_p, sz]),
             "vqe_create_hardware_efficient_ansatz": (C.c_void_p, [sz, sz]),
+            "vqe_create_uccsd_ansatz": (C.c_void_p, [sz, sz]),
+            "vqe_create_symmetry_preserving_ansatz": (C.c_void_p, [sz, sz, sz]),
+            "vqe_compute_gradient": (i, [C.c_void_p, C.POINTER(d), C.POINTER(d)]),
+            "moonlab_vqe_natural_gradient": (i, [C.c_void_p, C.POINTER(d), C.POINTER(d), d, C.POINTER(d), sz]),
             "vqe_optimizer_create": (C.c_void_p, [i]),
             "vqe_solver_create": (C.c_void_p, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
             "vqe_solver_free": (None, [C.c_void_p]),
@@ -240,6 +251,14 @@ def ref():
             "moonlab_vqe_berry_curvature": (i, [C.c_void_p, C.POINTER(d), C.POINTER(d), sz]),
             "vqe_natural_gradient_direction": (i, [C.c_void_p, C.POINTER(d), C.POINTER(d), d, C.POINTER(d)]),
         }
+        for k in ("h", "x", "y", "z", "s", "sdg", "t", "tdg"):
+            sigs[f"fuse_append_{k}"] = (i, [C.c_void_p, i])
+        for k in ("phase", "rx", "ry", "rz"):
+            sigs[f"fuse_append_{k}"] = (i, [C.c_void_p, i, d])
+        for k in ("cnot", "cz", "cy", "swap"):
+            sigs[f"fuse_append_{k}"] = (i, [C.c_void_p, i, i])
+        for k in ("cphase", "crx", "cry", "crz"):
+            sigs[f"fuse_append_{k}"] = (i, [C.c_void_p, i, i, d])
         for name, (res, args) in sigs.items():
             f = getattr(lib, name)
             f.restype = res
@@ -390,9 +409,11 @@ def ref_circuit_roundtrip(raw: bytes, explicit_len: bool = True):
 
 
 class RefSolver:
-    """A vqe_solver_t built through the reference API (HEA ansatz)."""
+    """A vqe_solver_t built through the reference API: the hardware-efficient
+    ansatz with `layers` layers, or ansatz=("uccsd", electrons) /
+    ("symmetry", occupied, layers)."""
 
-    def __init__(self, n: int, layers: int, paulis, coeffs, hf_reference: int = 0):
+    def __init__(self, n: int, layers: int, paulis, coeffs, hf_reference: int = 0, ansatz=None):
         L = self.lib = ref()
         self.h = L.pauli_hamiltonian_create(n, len(paulis))
         for k, (ps, c) in enumerate(zip(paulis, coeffs)):
@@ -403,11 +424,23 @@ class RefSolver:
             # num_qubits, num_terms, terms, nuclear_repulsion, molecule_name,
             # bond_distance: byte offset 48
             C.c_uint64.from_address(self.h + 48).value = hf_reference
-        self.ans = L.vqe_create_hardware_efficient_ansatz(n, layers)
+        if ansatz is None:
+            self.ans = L.vqe_create_hardware_efficient_ansatz(n, layers)
+        elif ansatz[0] == "uccsd":
+            self.ans = L.vqe_create_uccsd_ansatz(n, ansatz[1])
+        elif ansatz[0] == "symmetry":
+            self.ans = L.vqe_create_symmetry_preserving_ansatz(n, ansatz[1], ansatz[2])
+        else:
+            raise ValueError(ansatz)
+        if not self.ans:
+            raise RuntimeError(f"ansatz {ansatz} not created")
         self.opt = L.vqe_optimizer_create(2)  # any optimizer; vqe_solver_create needs one
         self.ctx = EntropyCtx(ENTROPY_FN(lambda ud, buf, sz: 0), None)
         self.solver = L.vqe_solver_create(self.h, self.ans, self.opt, C.byref(self.ctx))
-        self.P = 2 * n * layers
+        # vqe_ansatz_t.num_parameters (vqe.h:229-236): type (int, padded), num_qubits, num_layers, then it
+        self.P = C.c_size_t.from_address(self.ans + 24).value
+        if ansatz is None:
+            assert self.P == 2 * n * layers
 
     def gradient(self, params) -> np.ndarray:
         p = np.ascontiguousarray(params, dtype=np.float64)
@@ -432,6 +465,16 @@ class RefSolver:
     def berry_curvature(self, params) -> np.ndarray:
         """moonlab_vqe_berry_curvature: F = -2 Im Q."""
         return self._tensor(self.lib.moonlab_vqe_berry_curvature, params)
+
+    def natural_gradient(self, params, gradient, regularization: float) -> np.ndarray:
+        """moonlab_vqe_natural_gradient (the stable verb)."""
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        gr = np.ascontiguousarray(gradient, dtype=np.float64)
+        out = np.empty(self.P, dtype=np.float64)
+        rc = self.lib.moonlab_vqe_natural_gradient(self.solver, _dp(p), _dp(gr), regularization, _dp(out), self.P)
+        if rc:
+            raise RuntimeError(f"moonlab_vqe_natural_gradient: {rc}")
+        return out
 
     def natural_gradient_direction(self, params, gradient, regularization: float) -> np.ndarray:
         p = np.ascontiguousarray(params, dtype=np.float64)
