@@ -135,3 +135,27 @@ def test_small_requests_share_launches(gpu):
             assert B.port().svo_qgtl_execute(n, sv, len(sv), shots, seed,
                                               want.ctypes.data_as(C.POINTER(C.c_uint64)), None) == 0
             assert np.array_equal(out, want)
+
+
+@pytest.mark.gpu
+def test_larger_complex128_requests_match_the_oracle(gpu):
+    """Requests of the serving stream's shape up to 22 qubits (complex128):
+    outcomes bit-identical to the oracle's moonlab_qgtl_execute restatement,
+    alone and when they share the device with others."""
+    from moonlab_b200.serving import Server, request_circuit
+    reqs = [Request(i, 0.0, n, d, shots, 0, seed) for i, (n, d, shots, seed) in
+            enumerate([(18, 30, 200, 0x5A1), (20, 16, 128, 0x5A2), (21, 12, 96, 0x5A3), (22, 10, 64, 0x5A4),
+                       (22, 14, 33, 0x5A5)])]
+    circ = [request_circuit(r) for r in reqs]
+    with Server(workers=4) as s:
+        tickets = [s.submit(r.n, g, r.shots, r.seed, "c128") for r, g in zip(reqs, circ)]
+        mixed = [s.wait(t)[0] for t in tickets]
+    with Server(workers=1) as s:
+        alone = [s.wait(s.submit(r.n, g, r.shots, r.seed, "c128"))[0] for r, g in zip(reqs, circ)]
+    for r, g, a, b in zip(reqs, circ, alone, mixed):
+        assert np.array_equal(a, b)
+        want = np.empty(r.shots, dtype=np.uint64)
+        sv = B.to_svo(g)
+        assert B.port().svo_qgtl_execute(r.n, sv, len(sv), r.shots, r.seed,
+                                          want.ctypes.data_as(C.POINTER(C.c_uint64)), None) == 0
+        assert np.array_equal(a, want)
