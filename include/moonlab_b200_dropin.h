@@ -188,6 +188,12 @@ int fuse_append_cry(fuse_circuit_t *c, int ctrl, int tgt, double theta);
 int fuse_append_crz(fuse_circuit_t *c, int ctrl, int tgt, double theta);
 fuse_circuit_t *fuse_compile(const fuse_circuit_t *src, fuse_stats_t *stats);
 qs_error_t fuse_execute(const fuse_circuit_t *c, quantum_state_t *state);
+/* The engine ops fuse_execute queues for a fusion circuit on num_qubits
+ * qubits: ops is an mlb_op_t array of `capacity` records (moonlab_b200.h), or
+ * NULL to count only into *num_ops.  No counterpart in the reference: for
+ * callers that keep their own engine states (mlb_apply_ops). */
+int mlb_fuse_circuit_ops(const fuse_circuit_t *c, uint32_t num_qubits, void *ops, size_t capacity,
+                         size_t *num_ops);
 
 /* ---- scheduler backend plug-in (src/distributed/scheduler.h:225-262,
  *      registry scheduler.c:283-305).

@@ -128,12 +128,15 @@ int add2(fuse_circuit_t* c, int kind, int a, int b, double p0) {
 
 // One fuse record as engine ops (appended to out); false if unknown.
 bool to_ops(const fuse_gate_t& g, uint32_t n, std::vector<mlb_op_t>& out) {
-  if (g.kind == FUSE_GATE_FUSED_1Q || g.kind == FUSE_GATE_U3) {
-    const M2 m = matrix_of(g);
+  if (g.kind == FUSE_GATE_FUSED_1Q || g.kind == FUSE_GATE_U3 || g.kind == FUSE_GATE_CY) {
+    // CY is gate_cy's controlled Y (gates.c:670-697), not the QGTL record's
+    // S . CNOT . Sdg composition
+    const M2 m = g.kind == FUSE_GATE_CY ? M2{{{0.0, cd(0.0, -1.0)}, {cd(0.0, 1.0), 0.0}}} : matrix_of(g);
     mlb_op_t o{};
     o.kind = MLB_OP_1Q;
-    o.target = g.q[0];
+    o.target = g.kind == FUSE_GATE_CY ? g.q[1] : g.q[0];
     o.target2 = -1;
+    if (g.kind == FUSE_GATE_CY) o.cmask = 1ull << g.q[0];
     for (int i = 0; i < 2; i++)
       for (int j = 0; j < 2; j++) {
         o.m[2 * (2 * i + j)] = m.m[i][j].real();
@@ -143,7 +146,7 @@ bool to_ops(const fuse_gate_t& g, uint32_t n, std::vector<mlb_op_t>& out) {
     return true;
   }
   // gate records (QGTL numbering and its extensions, include/moonlab_b200.h)
-  static const int type_of[] = {4, 1, 2, 3, 5, 20, 6, 21, 22, 7, 8, 9, -1, -1, 10, 12, 11, 13, 23, 24, 25, 26};
+  static const int type_of[] = {4, 1, 2, 3, 5, 20, 6, 21, 22, 7, 8, 9, -1, -1, 10, 12, -1, 13, 23, 24, 25, 26};
   if (g.kind < 0 || g.kind > FUSE_GATE_CRZ || type_of[g.kind] < 0) return false;
   mlb_gate_t rec{};
   rec.type = type_of[g.kind];
@@ -259,6 +262,21 @@ fuse_circuit_t* fuse_compile(const fuse_circuit_t* src, fuse_stats_t* stats) {
     }
   if (stats) stats->fused_gates = dst->gates.size();
   return dst;
+}
+
+int mlb_fuse_circuit_ops(const fuse_circuit_t* c, uint32_t num_qubits, void* ops, size_t capacity,
+                         size_t* num_ops) {
+  if (!c || !num_ops) return MLB_ERR_INVALID_ARG;
+  if (num_qubits < c->n) return MLB_ERR_NUM_QUBITS;
+  std::vector<mlb_op_t> v;
+  for (const fuse_gate_t& g : c->gates)
+    if (!to_ops(g, num_qubits, v)) return MLB_ERR_INVALID_ARG;
+  *num_ops = v.size();
+  if (ops) {
+    if (capacity < v.size()) return MLB_ERR_INVALID_ARG;
+    std::memcpy(ops, v.data(), v.size() * sizeof(mlb_op_t));
+  }
+  return MLB_OK;
 }
 
 qs_error_t fuse_execute(const fuse_circuit_t* c, quantum_state_t* state) {

@@ -110,6 +110,37 @@ def test_compile_matches_the_reference(n, length, seed):
             lib.fuse_circuit_free(c)
 
 
+@pytest.mark.parametrize("n,length,seed,fused", [(5, 200, 21, True), (7, 300, 22, False), (8, 400, 23, True)])
+def test_lowered_ops_match_the_reference_execute(n, length, seed, fused):
+    """fuse_execute's engine ops (mlb_fuse_circuit_ops), replayed in numpy
+    with the engine's op semantics, equal the reference's fuse_execute on a
+    host state: every record kind, fused or not, mapped right."""
+    from test_tile_plan import apply_op
+    (lo, co, fo, _, _), (lr, cr, fr, _, _) = compile_both(n, random_program(n, length, seed))
+    try:
+        lib = _lib.load()
+        lib.mlb_fuse_circuit_ops.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t,
+                                             C.POINTER(C.c_size_t)]
+        src = fo if fused else co
+        cnt = C.c_size_t()
+        assert lib.mlb_fuse_circuit_ops(src, n, None, 0, C.byref(cnt)) == 0
+        ops = (_lib.MlbOp * cnt.value)()
+        assert lib.mlb_fuse_circuit_ops(src, n, ops, cnt.value, C.byref(cnt)) == 0
+        got = np.zeros(1 << n, dtype=np.complex128)
+        got[0] = 1
+        for o in ops:
+            apply_op(got, n, o)
+        want_s = B.RefStateVector(n)
+        assert lr.fuse_execute(fr if fused else cr, C.byref(want_s.s)) == 0
+        want = want_s.amplitudes()
+        want_s.close()
+        assert np.abs(got - want).max() < 1e-12
+    finally:
+        for lib_, c, f in ((lo, co, fo), (lr, cr, fr)):
+            lib_.fuse_circuit_free(f)
+            lib_.fuse_circuit_free(c)
+
+
 def test_validation_matches_the_reference():
     for lib in (_bind(_lib.load()), _bind(B.ref())):
         assert not lib.fuse_circuit_create(0) and not lib.fuse_circuit_create(33)
