@@ -67,16 +67,15 @@ def fp64_tensor_peak(local: int):
 
 def profiled_traffic(n: int):
     """DRAM bytes of one k_tile<double> pass at n qubits: the ncu figure of
-    bytes per amplitude (profiles/k_tile_c128_26q.md, dram read + write of
-    a 26-qubit pass) times 2^n.  A pass moves every amplitude once each way,
-    so its traffic grows in proportion to 2^n.  None if the summary is gone."""
-    p = ROOT / "profiles" / "k_tile_c128_26q.md"
+    bytes per amplitude (profiles/k_tile_c128_traffic.json, dram read + write
+    of a 26-qubit pass, from the capture summarised in
+    profiles/k_tile_c128_26q.md) times 2^n.  A pass moves every amplitude once
+    each way, so its traffic grows in proportion to 2^n.  None if the file is
+    gone."""
+    p = ROOT / "profiles" / "k_tile_c128_traffic.json"
     if not p.exists():
         return None
-    for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_amplitude_per_pass:"):
-            return float(line.split(":")[1]) * (1 << n)
-    return None
+    return float(json.loads(p.read_text())["dram_bytes_per_amplitude_per_pass"]) * (1 << n)
 
 
 class ClockSampler:
@@ -133,48 +132,92 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# reference CPU path: stratified per-gate sample of the circuit
+# reference CPU path: per-gate samples of the circuit, every target covered
 # ---------------------------------------------------------------------------
-def reference_sample(n: int, budget_s: float, gates):
-    """Time the reference library's gate_* calls at n qubits on a stratified
-    sample (each gate type at low / middle / high targets) and extrapolate
-    the full circuit.  Returns (circuit_seconds, sample_description, cores,
-    kind)."""
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    from oracle import bindings as B
-    if B.have_ref():
-        r = B.RefStateVector(n)
-        kind = "reference"
-    else:
-        raise RuntimeError("reference library oracle/_ref/liboracle.so not built")
-    L, p = r.lib, C.byref(r.s)
-    targets = [0, 1, n // 2, n - 2]
-    kinds = {
-        "rx": lambda q: L.gate_rx(p, q, 0.3), "ry": lambda q: L.gate_ry(p, q, 0.4),
-        "rz": lambda q: L.gate_rz(p, q, 0.5), "cnot": lambda q: L.gate_cnot(p, q, q + 1),
-    }
-    per = {}
-    t_start = time.perf_counter()
-    reps = 0
-    while True:
-        for k, f in kinds.items():
-            for q in targets:
-                t0 = time.perf_counter()
-                f(q)
-                per.setdefault(k, []).append(time.perf_counter() - t0)
-        reps += 1
-        if time.perf_counter() - t_start > budget_s or reps >= 4:
-            break
-    mean = {k: sum(v) / len(v) for k, v in per.items()}
-    counts = {k: int(np.sum(gates["type"] == t)) for k, t in (("rx", 7), ("ry", 8), ("rz", 9), ("cnot", 10))}
-    nzz = int(np.sum(gates["type"] == 27))
-    total = sum(mean[k] * counts[k] for k in counts) + nzz * (2 * mean["cnot"] + mean["rz"])
-    sample = (f"{reps * len(targets) * len(kinds)} gate_* calls at {n} qubits (RX/RY/RZ/CNOT at "
-              f"targets {targets}), {time.perf_counter() - t_start:.1f} s; circuit time extrapolated "
-              f"per gate over {len(gates)} gates (ZZ = CNOT.RZ.CNOT)")
-    r.close()
-    return total, sample, int(os.environ.get("OMP_NUM_THREADS", cores)), kind
+class ReferenceSampler:
+    """Times the reference library's gate_* calls at n qubits and
+    extrapolates the whole circuit from the circuit's own histogram of
+    (gate type, target) pairs: RX / RY / RZ at every target 0..n-1 and
+    CNOT(q, q+1) at every q (ZZ = CNOT.RZ.CNOT, qaoa.c:745-753).  The
+    reference threads a gate only when the state has >= 2^18 amplitudes and
+    >= 32 blocks above the target (gates.c:121, 137-140), so per-target times
+    differ and every target is sampled: each step times the next pairs of a
+    fixed rotation until its time budget is spent, and a pair's time is the
+    mean of all its samples so far (a pair not yet sampled takes its gate
+    type's mean)."""
+
+    def __init__(self, n: int, gates):
+        cores = os.cpu_count() or 1
+        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+        self.cores = int(os.environ.get("OMP_NUM_THREADS", cores))
+        from oracle import bindings as B
+        if not B.have_ref():
+            raise RuntimeError("reference library oracle/_ref/liboracle.so not built")
+        self.kind = "reference"
+        self.r = B.RefStateVector(n)
+        L, p = self.r.lib, C.byref(self.r.s)
+        self.n = n
+        self.call = {"rx": lambda q: L.gate_rx(p, q, 0.3), "ry": lambda q: L.gate_ry(p, q, 0.4),
+                     "rz": lambda q: L.gate_rz(p, q, 0.5), "cnot": lambda q: L.gate_cnot(p, q, q + 1)}
+        # the circuit's (type, target) histogram; CNOT keyed by its control q (target q + 1)
+        self.count = {}
+        for g in gates:
+            t, tgt, ctl = int(g["type"]), int(g["target"]), int(g["control"])
+            keys = {7: [("rx", tgt)], 8: [("ry", tgt)], 9: [("rz", tgt)], 10: [("cnot", ctl)],
+                    27: [("cnot", ctl), ("rz", tgt), ("cnot", ctl)]}[t]
+            for k in keys:
+                self.count[k] = self.count.get(k, 0) + 1
+        # targets in bit-reversed order, so every prefix of the rotation spreads
+        # over low, middle and high targets (and the threaded / serial regimes)
+        nb = max(1, (n - 1).bit_length())
+        spread = sorted(range(n), key=lambda q: int(format(q, f"0{nb}b")[::-1], 2))
+        self.pairs = [(k, q) for q in spread for k in ("rx", "ry", "rz", "cnot") if k != "cnot" or q < n - 1]
+        self.samples = {}
+        self.next = 0
+        self.calls = 0
+
+    def step(self, budget_s: float) -> float:
+        t_start = time.perf_counter()
+        done = 0
+        while done < 4 or time.perf_counter() - t_start < budget_s:
+            k, q = self.pairs[self.next % len(self.pairs)]
+            self.next += 1
+            t0 = time.perf_counter()
+            self.call[k](q)
+            self.samples.setdefault((k, q), []).append(time.perf_counter() - t0)
+            done += 1
+        self.calls += done
+        by_kind = {}
+        for (k, _), v in self.samples.items():
+            by_kind.setdefault(k, []).extend(v)
+        kind_mean = {k: sum(v) / len(v) for k, v in by_kind.items()}
+        total = 0.0
+        for (k, q), c in self.count.items():
+            v = self.samples.get((k, q))
+            total += c * (sum(v) / len(v) if v else kind_mean.get(k, max(kind_mean.values())))
+        return total
+
+    def describe(self) -> str:
+        covered = sum(1 for pq in self.pairs if pq in self.samples)
+        return (f"{self.calls} gate_* calls at {self.n} qubits so far, rotating over all {len(self.pairs)} "
+                f"(type, target) pairs of the circuit (RX/RY/RZ at every target, CNOT(q, q+1) at every q; "
+                f"{covered} covered); circuit time = sum over the circuit's {sum(self.count.values())} "
+                f"gate calls (ZZ = CNOT.RZ.CNOT) of its pair's mean time")
+
+    def close(self):
+        self.r.close()
+
+
+def reference_sample(n: int, budget_s: float, gates, rounds: int = 1):
+    """Circuit seconds from `rounds` sampler steps (the CPU baseline of the
+    B200 line); returns (seconds, sample, cores, kind)."""
+    smp = ReferenceSampler(n, gates)
+    try:
+        for _ in range(rounds):
+            secs = smp.step(budget_s)
+        return secs, smp.describe(), smp.cores, smp.kind
+    finally:
+        smp.close()
 
 
 # ---------------------------------------------------------------------------
@@ -206,13 +249,14 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return
     gates, _ = config_c2(args.qubits, args.depth)
+    smp = ReferenceSampler(args.qubits, gates)
     step_vals = []
-    samples = []
     for i in range(args.warmup + args.steps):
-        secs, sample, cores, kind = reference_sample(args.qubits, args.ref_budget, gates)
+        secs = smp.step(args.ref_budget)
         if i >= args.warmup:
             step_vals.append(secs)
-            samples.append(sample)
+    sample, cores, kind = smp.describe(), smp.cores, smp.kind
+    smp.close()
     secs = statistics.median(step_vals)
     val = 1.0 / secs
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "circuits/s", "n_gpus": args.gpus,
@@ -221,7 +265,7 @@ def run_reference(args, ws, rank):
             "data": "synthetic seeded circuit (splitmix64 0xC2)",
             "config": {"workload": WORKLOAD, "qubits": args.qubits, "depth": args.depth},
             "cpu_baseline": {"value": val, "unit": "circuits/s", "cores": cores, "kind": kind,
-                             "sample": samples[-1]},
+                             "sample": sample},
             "e2e": {"value": val, "unit": "circuits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -276,8 +320,9 @@ def run_b200(args, ws, rank, local):
     peak, peak_kind = measured_peaks()
     achieved = per_pass_bytes / avg_pass_s / 1e9
     # the dense segments' FP64 tensor-core work: a 16x16 complex matrix on
-    # every 16 amplitudes = 64 real multiply-adds (128 flops) per amplitude
-    dense_flops = dense_segments * 128.0 * (1 << n)
+    # every 16 amplitudes as three real 16x16 products (Gauss) = 48 real
+    # multiply-adds (96 flops) per amplitude
+    dense_flops = dense_segments * 96.0 * (1 << n)
 
     # the same c128 path with dense segments off: every register segment runs
     # gate by gate on the CUDA cores (no gate matrices multiplied together
@@ -355,10 +400,11 @@ def run_b200(args, ws, rank, local):
     fused["kernel"] = "k_fused"
 
     sv.close()
-    serving = None if args.no_serving else serving_leg(args, local,
-                                                       rank == 0 and ws == 1 and not args.no_cpu_baseline)
-    sweep = None if args.no_sweep else gate_sweep_leg(local, peak)
-    vqe = None if args.no_vqe else vqe_leg(local, rank == 0 and ws == 1 and not args.no_cpu_baseline)
+    # the serving, per-gate and VQE legs describe one GPU: run at N = 1 only
+    one = ws == 1
+    serving = None if args.no_serving or not one else serving_leg(args, local, not args.no_cpu_baseline)
+    sweep = None if args.no_sweep or not one else gate_sweep_leg(local, peak)
+    vqe = None if args.no_vqe or not one else vqe_leg(local, not args.no_cpu_baseline)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -412,16 +458,19 @@ def run_b200(args, ws, rank, local):
 
 
 def serving_leg(args, local, with_cpu: bool):
-    """The request stream (Poisson arrivals; qubits U{10..28}, depth
-    U{10..100}, shots U{1..4096}, dtype 50/50) on this rank's GPU through
-    the continuous-batching server: first all requests at once (capacity,
-    circuits/s), then paced at --serve-rate (latency p50/p99 at that load),
-    then 100 requests at each rate of a sweep, reporting the highest rate
-    whose p99 meets the stated target.  Latency = submit to result on the
-    host clock; circuits/s = requests / (last result - first submit).  With
-    with_cpu, the reference's moonlab_qgtl_execute is timed on the host on
-    up to 12 requests of <= 16 qubits beside the engine's time for the same
-    requests run one at a time."""
+    """The request stream of the serving workload (Poisson arrivals; qubits
+    U{10..28}, depth U{10..100}, shots U{1..4096}, dtype 50/50), all
+    --serve-requests of it (10,000 by default) paced at --serve-rate through
+    the continuous-batching server on this rank's GPU: circuits/s and p50/p99
+    latency at that load.  Beside it: the capacity (the first
+    --serve-capacity requests submitted at once) and a short arrival-rate
+    sweep (100 requests per rate) with the highest rate whose p99 meets the
+    stated target.  Latency = submit to result on the host clock; circuits/s
+    = requests / (last result - first submit).  With with_cpu, the
+    reference's moonlab_qgtl_execute (the control server's per-request path,
+    control_plane.c:688-716) is timed on the host on up to 12 requests of <=
+    16 qubits beside the engine's time for the same requests run one at a
+    time."""
     from moonlab_b200.circuits import config_c5
     from moonlab_b200.serving import Server, request_circuit, run_load
     reqs = config_c5(num=args.serve_requests, rate=args.serve_rate)
@@ -429,11 +478,12 @@ def serving_leg(args, local, with_cpu: bool):
     workers = 8
     p99_target_ms = 2000.0
     sweep = []
+    ncap = min(args.serve_capacity, len(reqs))
     with Server(device=local, workers=workers) as srv:
-        sat = run_load(srv, reqs, time_scale=0.0, circuits=circ)
+        sat = run_load(srv, reqs[:ncap], time_scale=0.0, circuits=circ[:ncap])
         paced = run_load(srv, reqs, time_scale=1.0, circuits=circ)
         # arrival-rate sweep: 100 requests of the stream re-timed at each rate
-        for lam in (8.0, 12.0, 16.0, 20.0):
+        for lam in (10.0, 20.0, 30.0, 40.0):
             sub = config_c5(num=100, rate=lam, seed=0xC5)
             sr = run_load(srv, sub, time_scale=1.0)
             sweep.append({"rate_per_s": lam, "circuits_per_s": sr["circuits_per_s"], "p50_ms": sr["p50_s"] * 1e3,
@@ -462,13 +512,16 @@ def serving_leg(args, local, with_cpu: bool):
                    "b200_mean_service_ms": 1e3 * sum(gpu_alone) / len(gpu_alone)}
         except Exception as e:  # reported, never replaced
             cpu = {"kind": "reference", "sample": f"unavailable: {e}"}
+    lat = np.array([info["latency_s"] for _, info in paced["results"]])
     return {
-        "workload": (f"{len(reqs)} requests of the Poisson stream (seed 0xC5): qubits U{{10..28}}, "
-                     "depth U{10..100} brickwork, shots U{1..4096}, c128/c64 50/50"),
-        "rate_per_s": args.serve_rate, "workers": workers,
+        "workload": (f"{len(reqs):,} requests of the Poisson stream (seed 0xC5) at {args.serve_rate:g}/s: "
+                     "qubits U{10..28}, depth U{10..100} brickwork, shots U{1..4096}, c128/c64 50/50"),
+        "rate_per_s": args.serve_rate, "workers": workers, "requests": len(reqs),
         "circuits_per_s": paced["circuits_per_s"], "p50_ms": paced["p50_s"] * 1e3,
         "p99_ms": paced["p99_s"] * 1e3, "mean_ms": paced["mean_s"] * 1e3,
-        "saturated_circuits_per_s": sat["circuits_per_s"], "saturated_p99_ms": sat["p99_s"] * 1e3,
+        "p999_ms": float(np.percentile(lat, 99.9)) * 1e3, "span_s": paced["span_s"],
+        "capacity": {"requests": ncap, "circuits_per_s": sat["circuits_per_s"], "p99_ms": sat["p99_s"] * 1e3,
+                     "how": f"the first {ncap} requests of the stream submitted at once"},
         "peak_running": paced["stats"]["peak_running"],
         "peak_reserved_gib": paced["stats"]["peak_reserved_bytes"] / 2**30,
         "p99_target_ms": p99_target_ms, "rate_sweep": sweep,
@@ -534,6 +587,7 @@ def vqe_leg(local, with_cpu: bool):
     prob = config_c4(n=20, layers=8, batch=256, seed=0xC4)
     res = {"workload": "HEA N=20 L=8 (320 parameters), 80 2-local Pauli terms, batch 256"}
     grads = {}
+    peak, peak_kind = measured_peaks()
     for dt in ("c128", "c64"):
         p = HEAProblem(20, 8, prob.coeffs, xmasks=prob.xmasks, zmasks=prob.zmasks, dtype=dt, device=local)
         p.evaluate(prob.params)  # warm-up at the full batch: workspaces are sized by the first call
@@ -544,8 +598,27 @@ def vqe_leg(local, with_cpu: bool):
             times.append(time.perf_counter() - t0)
         t = statistics.median(times)
         grads[dt] = G
+        # algorithmic bytes of one batch (per vector, S = one state's bytes):
+        # forward passes read + write psi (2 S each), the first lambda pass
+        # reads psi and writes lambda (2 S), later ones also read lambda (3 S),
+        # backward passes read + write psi and lambda (4 S each), and each
+        # checkpoint is saved and restored once (2 S + 2 S)
+        ps, ev = p.plan_stats(), p.last_eval_stats()
+        S = (16 if dt == "c128" else 8) << 20
+        ck = 0
+        if ev["checkpoints"]:
+            ck = -(-8 // ev["segment_layers"]) - 1  # segments - 1
+        per_vec = S * (2 * ps["forward_passes"] + 2 + 3 * (ps["lambda_passes"] - 1) + 4 * ps["backward_passes"]
+                       + 4 * ck)
+        achieved = per_vec * len(prob.params) / t / 1e9
         res[dt] = {"vectors_per_s": len(prob.params) / t, "batch_ms": t * 1e3,
-                   "timing": "median of 3 calls after a full-batch warm-up"}
+                   "timing": "median of 3 calls after a full-batch warm-up (host parameters in, host "
+                             "energies and gradients out)",
+                   "passes": ps, "checkpoints": ev,
+                   "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                "frac": achieved / peak, "peak_source": peak_kind,
+                                "algorithmic_bytes_per_vector": per_vec,
+                                "kernel": "k_adj_gates / k_adj_pauli (whole evaluation)"}}
         p.close()
     res["c64_max_rel_grad_err"] = float(np.abs(grads["c64"] - grads["c128"]).max() /
                                         max(1e-300, np.abs(grads["c128"]).max()))
@@ -591,8 +664,9 @@ def main():
     ap.add_argument("--depth", type=int, default=40)
     ap.add_argument("--ref-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=200)
-    ap.add_argument("--serve-rate", type=float, default=15.0)
+    ap.add_argument("--serve-requests", type=int, default=10000)
+    ap.add_argument("--serve-rate", type=float, default=25.0)
+    ap.add_argument("--serve-capacity", type=int, default=1000)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-sweep", action="store_true", help="skip the per-gate GB/s sweep")
     ap.add_argument("--no-vqe", action="store_true", help="skip the VQE adjoint-gradient leg")

@@ -1,10 +1,11 @@
 """Generate the committed golden fixtures from the reference itself.
 
-Run in a container that has the reference tree (the script reads its
-circuit corpus, tests/oracle/corpus/circuit_corpus.json) and the reference
-library built from its sources (oracle/Makefile -> oracle/_ref/liboracle.so):
+Run where the reference tree is (the script reads its circuit corpus,
+tests/oracle/corpus/circuit_corpus.json) and the reference library is built
+from its sources (oracle/Makefile -> oracle/_ref/liboracle.so); the tree is
+given by --reference or the MOONLAB_REFERENCE environment variable:
 
-    make -C oracle ref && python tests/golden/gen_golden.py
+    make -C oracle ref REF=<tree> && python tests/golden/gen_golden.py --reference <tree>
 
 (`python tests/golden/gen_golden.py circuit_text` writes only
 circuit_text.json.)  Every expected value below is produced by calling the
@@ -16,6 +17,7 @@ from __future__ import annotations
 
 import ctypes as C
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -27,7 +29,18 @@ sys.path.insert(0, str(REPO))
 from moonlab_b200.circuits import GATE_DTYPE, SplitMix64, brickwork, config_c4  # noqa: E402
 from oracle import bindings as B  # noqa: E402
 
-CORPUS = Path("/root/reference/tests/oracle/corpus/circuit_corpus.json")
+def reference_tree() -> Path:
+    """The reference tree: --reference PATH, else $MOONLAB_REFERENCE."""
+    args = sys.argv[1:]
+    if "--reference" in args:
+        return Path(args[args.index("--reference") + 1])
+    env = os.environ.get("MOONLAB_REFERENCE")
+    if not env:
+        raise SystemExit("give the reference tree: --reference PATH or MOONLAB_REFERENCE=PATH")
+    return Path(env)
+
+
+CORPUS_REL = Path("tests/oracle/corpus/circuit_corpus.json")
 OUT = Path(__file__).resolve().parent / "reference_golden.npz"
 NAME2TYPE = dict(x=1, y=2, z=3, h=4, s=5, t=6, rx=7, ry=8, rz=9, cnot=10, cz=12, swap=13,
                  sdg=20, tdg=21)
@@ -47,7 +60,7 @@ def corpus_gates(c) -> np.ndarray:
 def main() -> None:
     L = B.ref()
     out = {}
-    circuits = json.loads(CORPUS.read_text())["circuits"]
+    circuits = json.loads((reference_tree() / CORPUS_REL).read_text())["circuits"]
     ids, ns, offs, gates_all, amp_offs, amps_all = [], [], [0], [], [0], []
     samp_u = SplitMix64(0x601DE11).uniforms(256)
     samp_all, mall_all, ez_all, ex0, ey0, zz01 = [], [], [], [], [], []
@@ -203,7 +216,7 @@ def circuit_text() -> None:
 
 
 if __name__ == "__main__":
-    if sys.argv[1:] == ["circuit_text"]:
+    if "circuit_text" in sys.argv[1:]:
         circuit_text()
         sys.exit(0)
     main()
