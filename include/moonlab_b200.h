@@ -53,9 +53,10 @@ typedef enum {
 
 typedef enum { MLB_C128 = 0, MLB_C64 = 1 } mlb_dtype_t;
 
-/* Execution modes for queued gates. */
+/* Execution modes for queued gates.  A new state starts in MLB_EXEC_TILED
+ * (complex128) or MLB_EXEC_FUSED (complex64). */
 typedef enum {
-    MLB_EXEC_TILED = 0,  /* default: gates grouped into shared-memory tile passes */
+    MLB_EXEC_TILED = 0,  /* gates grouped into shared-memory tile passes */
     MLB_EXEC_EAGER = 1,  /* one full-state kernel per gate (the per-gate path) */
     MLB_EXEC_FUSED = 2   /* complex64 states: gates fused into dense k<=5-qubit blocks on the
                             tensor cores; states under 13 qubits and ops on more than 5 qubits
@@ -155,8 +156,11 @@ int  mlb_expect_pauli_sum(mlb_state_t *s, size_t num_terms, const uint64_t *xmas
  * Each call writes every scratch entry it reads; nothing needs clearing.
  * The first call on a device does a one-time set-up (it looks up the
  * array's address and the SM count); make that first call before any stream
- * capture on that device.  Errors: MLB_ERR_INVALID_ARG for null, misaligned
- * or non-device buffers and a bad dtype. */
+ * capture on that device.  The looked-up address belongs to the device's
+ * current context: the set-up does not survive cudaDeviceReset (or any
+ * other teardown of the primary context), after which this entry point must
+ * not be called again in the process.  Errors: MLB_ERR_INVALID_ARG for null,
+ * misaligned or non-device buffers and a bad dtype. */
 int  mlb_prob_one_all_noalloc(const void *amp_device, int dtype, uint32_t num_qubits,
                               double *out_device, void *stream);
 /* probability vector; rule 0 = cabs(a)^2 (measurement.c:140),
@@ -377,6 +381,15 @@ int  mlb_state_set_dense(mlb_state_t *s, int on);
 /* Record CUDA events around each flush's kernels on the state's stream;
  * mlb_last_flush_stats then reports their elapsed device time (synchronizes). */
 int  mlb_state_set_timing(mlb_state_t *s, int enable);
+/* Test hook for the fused path's bounded waits (complex64 states in
+ * MLB_EXEC_FUSED): the next fused flush runs its first pass with CTA 0's
+ * first operand-image copy not requested and every wait limited to 20 ms
+ * instead of 2 s.  That CTA's waits run out with no copy and no tensor-core
+ * work in flight, it frees its tensor memory and returns, and the flush's
+ * synchronize reports MLB_ERR_TIMEOUT; the state's contents are then
+ * undefined but the state and the device stay usable (reset and rerun).
+ * Queued ops are flushed first.  No counterpart in the reference. */
+int  mlb_test_fused_skip_copy(mlb_state_t *s);
 /* Plan ops exactly as a flush would, on the host only (no device needed):
  * reports the passes and algorithmic bytes a flush of these ops launches.
  * fuse1q != 0 applies a flush's op fusion first: runs of uncontrolled

@@ -135,6 +135,7 @@ _SIGS = {
     "mlb_run_gates": (C.c_int, [C.c_void_p, C.POINTER(MlbGate), C.c_size_t]),
     "mlb_last_flush_stats": (C.c_int, [C.c_void_p, C.POINTER(MlbFlushStats)]),
     "mlb_state_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "mlb_test_fused_skip_copy": (C.c_int, [C.c_void_p]),
     "mlb_state_set_plan_cache": (C.c_int, [C.c_void_p, C.c_size_t]),
     "mlb_state_set_dense": (C.c_int, [C.c_void_p, C.c_int]),
     "mlb_plan_ops": (C.c_int, [C.POINTER(MlbOp), C.c_size_t, C.c_uint32, C.c_int, C.c_int,

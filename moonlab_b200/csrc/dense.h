@@ -2,7 +2,7 @@
 // kernel, kernels_tile.cu).
 //
 // A register segment of a complex128 tile pass (planner.h) runs dense when it
-// fits: four register qubits in a 13-qubit tile, and at most kDenseMaxCond
+// fits: four register qubits in a 12-qubit tile, and at most kDenseMaxCond
 // conditioning qubits outside them (controls and diagonal keys of its ops,
 // tile-local or outside the tile).  Its ops are multiplied into one 16x16
 // complex matrix per value of the conditioning qubits, in FP64, by applying
@@ -164,12 +164,12 @@ struct SegPlan {
 inline bool plan_segment(const DevPass& P, const DevSegment& sg, const DevOp* ops, DenseSegDev& D, SegPlan& S) {
   uint32_t cl = 0;
   uint64_t co = 0;
-  if (P.L + P.H != 13 || !conditioning(sg, ops, cl, co)) return false;
+  if (P.L + P.H != kTileBitsC128 || !conditioning(sg, ops, cl, co)) return false;
   std::memset(&D, 0, sizeof D);
   uint32_t reg = 0;
   for (int b = 0; b < 4; b++) reg |= 1u << sg.bits[b];
   int nloc = 0, nout = 0;
-  for (int b = 0; b < 13; b++)
+  for (int b = 0; b < kTileBitsC128; b++)
     if (cl >> b & 1u) S.locbits[nloc++] = b;
   for (int b = 0; b < 64; b++)
     if (co >> b & 1ull) D.obit[nout++] = (uint8_t)b;
@@ -198,19 +198,19 @@ inline bool plan_segment(const DevPass& P, const DevSegment& sg, const DevOp* op
       }
   // group-index bits: three chosen free bits, the other free local bits, then
   // the conditioning ones (a run of 8 groups shares its conditioning values)
-  int free_bits[9], nfree = 0;
-  for (int b = 0; b < 13; b++)
+  int free_bits[kDenseGroupBits], nfree = 0;
+  for (int b = 0; b < kTileBitsC128; b++)
     if (!(reg >> b & 1u) && !(cl >> b & 1u)) free_bits[nfree++] = b;
-  bool used[9] = {false, false, false, false, false, false, false, false, false};
+  bool used[kDenseGroupBits] = {};
   auto pick = [&](int avoid) {  // a free bit whose bank-group bit is outside `avoid`
     for (int i = 0; i < nfree; i++)
       if (!used[i] && !(ub(free_bits[i]) & avoid)) { used[i] = true; return free_bits[i]; }
     for (int i = 0; i < nfree; i++)
       if (!used[i]) { used[i] = true; return free_bits[i]; }
-    return -1;  // not reached: at least 5 free bits
+    return -1;  // not reached: at least 4 free bits
   };
   const int u0 = ub(sg.bits[perm[0]]), u1 = ub(sg.bits[perm[1]]);
-  int gbits[9];
+  int gbits[kDenseGroupBits];
   gbits[0] = pick(u0 | u1);
   gbits[1] = pick(u0);
   gbits[2] = pick(u0 | ub(gbits[1]));
@@ -225,9 +225,9 @@ inline bool plan_segment(const DevPass& P, const DevSegment& sg, const DevOp* op
       if (c >> i & 1) e |= 1u << gbits[i];
     D.g_lo[c] = (uint16_t)tile_swz16(e);
   }
-  for (int h = 0; h < 64; h++) {
+  for (int h = 0; h < (1 << kDenseColBits); h++) {
     uint32_t e = 0;
-    for (int i = 0; i < 6; i++)
+    for (int i = 0; i < kDenseColBits; i++)
       if (h >> i & 1) e |= 1u << gbits[3 + i];
     D.g_hi[h] = (uint16_t)tile_swz16(e);
   }

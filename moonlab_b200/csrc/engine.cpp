@@ -113,6 +113,7 @@ struct mlb_state {
   int* d_ferr = nullptr;
   int* h_ferr = nullptr;
   bool ferr_pending = false;
+  bool test_skip_copy = false;  // mlb_test_fused_skip_copy: the next fused flush only
   // plan cache for repeated circuit shapes (tiled mode; 0 entries = off)
   struct PlanEntry {
     std::vector<uint64_t> shape;              // the fused ops' shape words
@@ -492,8 +493,11 @@ int flush_fused(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   const FusedBlockDev* d_blocks = reinterpret_cast<const FusedBlockDev*>(s->d_plan);
   const uint8_t* d_images = reinterpret_cast<const uint8_t*>(s->d_plan) + ioff;
   cudaMemsetAsync(s->d_ferr, 0, sizeof(int), s->stream);
+  const int skip = s->test_skip_copy ? 1 : 0;
+  s->test_skip_copy = false;
   for (const auto& dp : P.dev_passes) {
-    rc = launch_fused_pass(s->amp, (int)s->n, dp, d_blocks, d_images, s->d_ferr, s->num_sms, s->stream);
+    rc = launch_fused_pass(s->amp, (int)s->n, dp, d_blocks, d_images, s->d_ferr, s->num_sms, s->stream,
+                           &dp == &P.dev_passes[0] ? skip : 0);
     if (rc) return fail(rc, "fused pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     st.passes++;
     st.kernel_launches++;
@@ -614,8 +618,10 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   const double* d_frags = reinterpret_cast<const double*>((unsigned char*)s->d_plan + foff);
   auto launch_passes = [&]() -> int {
     for (const auto& pp : E->passes) {
+      bool all_dense = pp.pass.num_segments > 0;
+      for (int k = 0; k < pp.pass.num_segments; k++) all_dense = all_dense && dev_segs[pp.seg_begin + k].mode == 2;
       const int r = launch_tile_pass(s->dtype, s->amp, pp.pass, d_segs + pp.seg_begin, d_ops, d_dsegs, d_frags,
-                                     s->num_sms, s->stream);
+                                     s->num_sms, s->stream, all_dense);
       if (r) return r;
     }
     return MLB_OK;
@@ -800,6 +806,9 @@ int mlb_state_create(uint32_t n, int dtype, int device, mlb_state_t** out) {
   s->n = n;
   s->dtype = dtype;
   s->device = device;
+  // complex64 states run the fused tensor-core path by default (states under
+  // 13 qubits fall back to tile passes inside the flush)
+  s->mode = dtype == MLB_C64 ? MLB_EXEC_FUSED : MLB_EXEC_TILED;
   s->bytes = (size_t)(dtype == MLB_C128 ? 16 : 8) << n;
   cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
   cudaError_t e = cudaMalloc(&s->amp, s->bytes);
@@ -888,6 +897,16 @@ int mlb_state_stream(const mlb_state_t* s, void** out) {
   *out = (void*)s->stream;
   return MLB_OK;
 }
+int mlb_test_fused_skip_copy(mlb_state_t* s) {
+  if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
+  if (s->dtype != MLB_C64) return fail(MLB_ERR_NOT_SUPPORTED, "the fused path runs complex64 states");
+  DeviceGuard dg(s->device);
+  int rc = flush_impl(s);  // queued ops run as they were queued
+  if (rc) return rc;
+  s->test_skip_copy = true;
+  return MLB_OK;
+}
+
 int mlb_state_set_dense(mlb_state_t* s, int on) {
   if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
   DeviceGuard dg(s->device);

@@ -74,6 +74,7 @@ constexpr uint32_t kTmemCols = 256;  // D: columns 0..127 (64 per half); A: 128.
 constexpr uint32_t kACol = 128;      // A of half h: hi at kACol + 64 h, lo at kACol + 64 h + 32
 constexpr long long kWaitLimit = 1ll << 24;       // try_wait rounds before giving up (a backstop)
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // and 2 s of wall time
+constexpr uint64_t kTestWaitLimitNs = 20000000ull;  // 20 ms in the bounded-wait test mode
 constexpr uint32_t kWaitHintNs = 100000;          // suspend-time hint of one try_wait
 
 // instruction descriptor: D = F32, A = B = BF16, both K-major, N = 64, M = 128
@@ -148,13 +149,13 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   return t;
 }
 
-// Bounded by time: false after kWaitLimitNs without the phase completing.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+// Bounded by time: false after limit_ns without the phase completing.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
   if (mbar_try(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   for (long long i = 0; i < kWaitLimit; i++) {
     if (mbar_try(bar, parity)) return true;
-    if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
   return false;
 }
@@ -218,9 +219,13 @@ __device__ __forceinline__ uint64_t tile_global(uint64_t gbase, uint32_t e, cons
   return g;
 }
 
+// test_skip_copy: CTA 0 does not request its first operand image (and waits
+// give up after kTestWaitLimitNs), so its first block's waits run out with no
+// copy and no MMA in flight -- the bounded-wait test of mlb_test_fused_skip_copy.
 __global__ void __launch_bounds__(kFThreads, 2)
     k_fused(float2* __restrict__ amp, FusedPassDev pass, const FusedBlockDev* __restrict__ blocks,
-            const uint8_t* __restrict__ images, int* __restrict__ err) {
+            const uint8_t* __restrict__ images, int* __restrict__ err, int test_skip_copy) {
+  const uint64_t wait_ns = test_skip_copy ? kTestWaitLimitNs : kWaitLimitNs;
   extern __shared__ uint8_t smraw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
   const uint32_t sbase = smem_u32(sm);
@@ -285,7 +290,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
 
   uint32_t ph_mma = 0, ph_b = 0;
   bool bad = false;
-  if (tid == 0 && (uint64_t)blockIdx.x < pass.num_tiles)
+  if (tid == 0 && (uint64_t)blockIdx.x < pass.num_tiles && !(test_skip_copy && blockIdx.x == 0))
     bulk_load(sbase + kBHi, images + (size_t)imgtab[0] * 16384, 16384, bar_b);
   float2* tile = reinterpret_cast<float2*>(sm + kTile0);
   // A tile's loads are issued by the previous tile's store loop (each thread
@@ -365,7 +370,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
       if (half == 0) asm volatile("bar.sync 1, 128;\n" ::: "memory");
       else asm volatile("bar.sync 2, 128;\n" ::: "memory");
       if (tid == 0 || tid == 160) {
-        if (mbar_wait_bounded(bar_b, ph_b)) {  // operand image landed
+        if (mbar_wait_bounded(bar_b, ph_b, wait_ns)) {  // operand image landed
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
           const uint32_t a_h = tmem + kACol + half * 64u, d_h = tmem + half * 64u;
 #pragma unroll
@@ -388,8 +393,8 @@ __global__ void __launch_bounds__(kFThreads, 2)
         int ok = 0;
         __syncwarp();
         if (lane == 0 && !*flag) {
-          ok = mbar_wait_bounded(bar_mma + 8u * half, ph_mma) ? 1 : 0;
-          if (ok && warp == 5) ok = mbar_wait_bounded(bar_mma, ph_mma) ? 1 : 0;  // and half 0
+          ok = mbar_wait_bounded(bar_mma + 8u * half, ph_mma, wait_ns) ? 1 : 0;
+          if (ok && warp == 5) ok = mbar_wait_bounded(bar_mma, ph_mma, wait_ns) ? 1 : 0;  // and half 0
           if (!ok) atomicOr((int*)flag, 2);
           if (ok && warp == 5) {
             const bool more = b + 1 < pass.num_blocks || t + gridDim.x < pass.num_tiles;
@@ -461,10 +466,10 @@ __global__ void __launch_bounds__(kFThreads, 2)
   if (bad && tid == 0) {  // flag bit 1: an operand copy may be pending
     atomicExch(err, 1);
     const int f = *flag;
-    if (f & 1) mbar_wait_bounded(bar_b, ph_b);
+    if (f & 1) mbar_wait_bounded(bar_b, ph_b, wait_ns);
     // either half's MMAs may be in flight (the halves have separate issuers)
-    mbar_wait_bounded(bar_mma, ph_mma);
-    mbar_wait_bounded(bar_mma + 8, ph_mma);
+    mbar_wait_bounded(bar_mma, ph_mma, wait_ns);
+    mbar_wait_bounded(bar_mma + 8, ph_mma, wait_ns);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
@@ -475,7 +480,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
 }  // namespace
 
 int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,
-                      const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream) {
+                      const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream, int test_skip_copy) {
   if (n < 13 || pass.num_blocks == 0 || pass.num_blocks > (uint32_t)kMaxBlocks ||
       pass.num_low < 1 || pass.num_low + pass.num_high != 13)
     return MLB_ERR_INVALID_ARG;
@@ -490,7 +495,7 @@ int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlo
   uint64_t grid = (uint64_t)num_sms * 2;  // two CTAs per SM
   if (grid > pass.num_tiles) grid = pass.num_tiles;
   k_fused<<<(unsigned)grid, kFThreads, kSmemBytes, stream>>>(reinterpret_cast<float2*>(amp), pass, d_blocks,
-                                                             d_images, d_err);
+                                                             d_images, d_err, test_skip_copy);
   count_launch();
   return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
 }

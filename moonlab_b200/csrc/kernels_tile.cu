@@ -42,13 +42,18 @@ namespace mlb {
 namespace {
 
 template <typename Real> struct TileCfg;
-template <> struct TileCfg<double> {  // complex128: 2^13 amps = 128 KiB per CTA (one CTA per SM)
-  static constexpr int TB = 13, RB = 4, NT = 256, MINB = 1, SW_SHIFT = 3, SW_MASK = 7, GPT = 1;
+template <> struct TileCfg<double> {  // complex128: 2^12 amps = 64 KiB per CTA, two CTAs of 4 warps per SM
+  static constexpr int TB = kTileBitsC128, RB = 4, NT = 128, MINB = 2, SW_SHIFT = 3, SW_MASK = 7, GPT = 1;
+  static constexpr int LOW = kLowBitsC128;
 };
 template <> struct TileCfg<float> {   // complex64: 2^13 amps = 64 KiB per CTA
   static constexpr int TB = 13, RB = 4, NT = 256, MINB = 2, SW_SHIFT = 4, SW_MASK = 15, GPT = 1;
+  static constexpr int LOW = 5;
 };
-// GPT: register groups per thread per segment, interleaved for ILP.
+// GPT: register groups per thread per segment, interleaved for ILP.  LOW:
+// contiguous low qubits of a tile of a state larger than one tile (rows).
+// Two complex128 CTAs per SM run independent tile sequences, so one CTA's
+// loads and stores overlap the other's tensor-core work.
 
 template <typename Real>
 __device__ __forceinline__ uint32_t swz(uint32_t e) {
@@ -212,19 +217,23 @@ __device__ __forceinline__ int dense_variant(const DenseSegDev* __restrict__ sg,
   const int nloc = sg->nloc, nout = sg->nout;
   uint32_t vout = 0;
   for (int k = 0; k < nout; k++) vout |= (uint32_t)((tile_base >> sg->obit[k]) & 1ull) << k;
-  return (nloc ? (j >> (6 - nloc)) : 0) | (int)(vout << nloc);
+  return (nloc ? (j >> (kDenseColBits - nloc)) : 0) | (int)(vout << nloc);
 }
 
 // pf: this warp's first matrix variant of the segment, loaded by the previous
 // dense segment (have_pf); nsg / nbase: the next dense segment and its tile,
 // whose first variant this call loads into pf during its last step, so the
 // L2 latency of the fragments overlaps that step and the barrier.
-template <int NT>
+// PIPE (passes whose segments all run dense): the next step's operands are
+// loaded before this step's DMMAs, so their shared-memory latency overlaps
+// the tensor-core work; the kernel that also holds gate-by-gate segments
+// keeps the loads in the step (its registers are spent on those).
+template <int NT, bool PIPE>
 __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const DenseSegDev* __restrict__ sg,
                                               const double* __restrict__ frags, uint64_t tile_base,
                                               bool have_pf, double (&pf)[16],
                                               const DenseSegDev* __restrict__ nsg, uint64_t nbase) {
-  constexpr int kWarps = NT / 32, kPerWarp = 64 / kWarps;  // 64 column tiles of 8 groups
+  constexpr int kWarps = NT / 32, kPerWarp = (1 << kDenseColBits) / kWarps;  // column tiles of 8 groups
   // warp w takes column tiles kPerWarp w .. + kPerWarp - 1: their conditioning
   // values (the top group-index bits) rarely change within a warp
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g8 = lane >> 2, q = lane & 3;
@@ -238,7 +247,8 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
   const uint32_t glb = sg->g_lo[g8], gld0 = sg->g_lo[2 * q], gld1 = sg->g_lo[2 * q + 1];
   const double* fseg = frags + sg->frag_off + lane;
   int cur = -1;
-  double ar[8], aj[8], as[8];  // fragment (i, s) at index 4 i + s
+  double ar[8], aj[8];  // fragment (i, s) at index 4 i + s
+  double2 x0[4], x1[4];        // this step's B operands (two column tiles)
   // two column tiles per step: 12 independent accumulator chains per warp
   // cover the DMMA latency; they differ only in bit 0 of j, so they share
   // their conditioning values (the top nloc <= 5 of j's 6 bits)
@@ -246,7 +256,7 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
   for (int u = 0; u < kPerWarp; u += 2) {
     const int j = kPerWarp * warp + u;  // column tiles j, j + 1: groups 8 j .. 8 j + 15
     const uint32_t ghi0 = sg->g_hi[j], ghi1 = sg->g_hi[j + 1];
-    const int var = (nloc ? (j >> (6 - nloc)) : 0) | (int)(vout << nloc);
+    const int var = (nloc ? (j >> (kDenseColBits - nloc)) : 0) | (int)(vout << nloc);
     if (var != cur) {  // warp-uniform
       if (u == 0 && have_pf) {
 #pragma unroll
@@ -262,15 +272,25 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
           aj[k] = __ldg(f + 32 * (8 + k));
         }
       }
-#pragma unroll
-      for (int k = 0; k < 8; k++) as[k] = ar[k] + aj[k];
       cur = var;
     }
-    double2 x0[4], x1[4];
+    if (u == 0 || !PIPE) {
 #pragma unroll
-    for (int t4 = 0; t4 < 4; t4++) {
-      x0[t4] = sm[ghi0 ^ glb ^ boff[t4]];
-      x1[t4] = sm[ghi1 ^ glb ^ boff[t4]];
+      for (int t4 = 0; t4 < 4; t4++) {
+        x0[t4] = sm[ghi0 ^ glb ^ boff[t4]];
+        x1[t4] = sm[ghi1 ^ glb ^ boff[t4]];
+      }
+    }
+    // the next step's operands (column tiles j + 2, j + 3: groups no other
+    // step of this segment writes) are loaded before this step's DMMAs
+    double2 y0[4], y1[4];
+    if (PIPE && u + 2 < kPerWarp) {
+      const uint32_t nh0 = sg->g_hi[j + 2], nh1 = sg->g_hi[j + 3];
+#pragma unroll
+      for (int t4 = 0; t4 < 4; t4++) {
+        y0[t4] = sm[nh0 ^ glb ^ boff[t4]];
+        y1[t4] = sm[nh1 ^ glb ^ boff[t4]];
+      }
     }
     if (u == kPerWarp - 2 && nsg != nullptr) {  // last step: fetch the next segment's first variant
       const double* f = frags + nsg->frag_off + lane +
@@ -296,8 +316,9 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
         dmma_f64(t[1][0][i][0], t[1][0][i][1], ar[f], x1[sk].x);
         dmma_f64(t[0][1][i][0], t[0][1][i][1], aj[f], x0[sk].y);
         dmma_f64(t[1][1][i][0], t[1][1][i][1], aj[f], x1[sk].y);
-        dmma_f64(t[0][2][i][0], t[0][2][i][1], as[f], s0);
-        dmma_f64(t[1][2][i][0], t[1][2][i][1], as[f], s1);
+        const double af = ar[f] + aj[f];  // R + J (kept out of registers between steps)
+        dmma_f64(t[0][2][i][0], t[0][2][i][1], af, s0);
+        dmma_f64(t[1][2][i][0], t[1][2][i][1], af, s1);
       }
     }
     // in place: this warp's 16 groups are read above and by no other warp
@@ -313,10 +334,19 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
     sm[ghi1 ^ gld0 ^ doff1] = out(1, 1, 0);
     sm[ghi1 ^ gld1 ^ doff0] = out(1, 0, 1);
     sm[ghi1 ^ gld1 ^ doff1] = out(1, 1, 1);
+    if (PIPE && u + 2 < kPerWarp) {
+#pragma unroll
+      for (int t4 = 0; t4 < 4; t4++) {
+        x0[t4] = y0[t4];
+        x1[t4] = y1[t4];
+      }
+    }
   }
 }
 
-template <typename Real>
+// DENSE (complex128 passes whose segments all run dense): only the dense
+// segment code, pipelined; no op program to decode.
+template <typename Real, bool DENSE>
 __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
     k_tile(typename Cplx<Real>::T* __restrict__ amp, const DevPass pass,
            const DevSegment* __restrict__ segs, const DevOp* __restrict__ ops,
@@ -327,12 +357,13 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A* sm = reinterpret_cast<A*>(smem_raw);
   // global offsets of the tile's rows (its high-qubit combinations); rows
-  // are at least 2^kLowBitsC128 amplitudes long
-  __shared__ uint64_t rowoff[1 << (TileCfg<Real>::TB - (kLowBitsC128 < 5 ? kLowBitsC128 : 5))];
-  __shared__ SmOp sops[kMaxPassOps];
-  __shared__ A smat[kMaxPassOps][4];
-  __shared__ uint8_t ton[kMaxPassOps];
-  __shared__ uint8_t tkey[kMaxPassOps];
+  // are 2^LOW amplitudes long
+  __shared__ uint64_t rowoff[1 << (TileCfg<Real>::TB - TileCfg<Real>::LOW)];
+  constexpr int kProg = DENSE ? 1 : kMaxPassOps;  // the op program (gate-by-gate segments)
+  __shared__ SmOp sops[kProg];
+  __shared__ A smat[kProg][4];
+  __shared__ uint8_t ton[kProg];
+  __shared__ uint8_t tkey[kProg];
   __shared__ DevSegment ssegs[kMaxPassSegs];
 
   const int L = pass.L, H = pass.H;
@@ -355,7 +386,7 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
     sg.op_end -= op0;
     ssegs[s] = sg;
   }
-  for (int o = threadIdx.x; o < nops; o += NT) {
+  for (int o = threadIdx.x; o < (DENSE ? 0 : nops); o += NT) {
     const DevOp& d = ops[op0 + o];
     SmOp so;
     so.kind = (uint8_t)d.kind;
@@ -400,7 +431,7 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   for (uint64_t tile = blockIdx.x; tile < pass.num_tiles; tile += gridDim.x) {
     const uint64_t tile_base = pdep64(tile, pass.tile_free_mask);
     // tile-constant op predicates and keys
-    for (int o = threadIdx.x; o < nops; o += NT) {
+    for (int o = threadIdx.x; o < (DENSE ? 0 : nops); o += NT) {
       const DevOp& d = ops[op0 + o];
       bool on = (tile_base & d.ocmask) == d.ocmask;
       uint32_t key = 0;
@@ -445,8 +476,8 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
             nsg = dsegs + ssegs[0].dense;
             nbase = pdep64(tile + gridDim.x, pass.tile_free_mask);
           }
-          dense_segment<NT>(reinterpret_cast<double2*>(sm), dsegs + seg.dense, frags, tile_base, have_pf, pf,
-                            nsg, nbase);
+          dense_segment<NT, DENSE>(reinterpret_cast<double2*>(sm), dsegs + seg.dense, frags, tile_base, have_pf,
+                                   pf, nsg, nbase);
           have_pf = nsg != nullptr;
           __syncthreads();
           continue;
@@ -456,6 +487,7 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
 #pragma unroll
         for (int k = 0; k < 16; k++) pf[k] = 0.0;
       }
+      if constexpr (!DENSE) {
       if (seg.mode == 1) {
         const int o = seg.op_begin;
         if (ton[o]) smem_quad<Real>(sm, tile_amps, ops[op0 + o], NT);
@@ -523,6 +555,7 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
         }
       }
       __syncthreads();
+      }  // !DENSE
     }
 
     // shared -> HBM (streaming stores: the state is far larger than L2), and
@@ -572,12 +605,14 @@ void prepare_tile_t() {
   cudaGetDevice(&dev);
   const uint64_t bit = 1ull << (dev & 63);
   if (!(attr_set_mask.load(std::memory_order_acquire) & bit)) {
-    cudaFuncSetAttribute(k_tile<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    cudaFuncSetAttribute(k_tile<Real, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    if constexpr (sizeof(Real) == 8)
+      cudaFuncSetAttribute(k_tile<Real, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
     attr_set_mask.fetch_or(bit, std::memory_order_release);
   }
 }
 
-template <typename Real>
+template <typename Real, bool DENSE>
 int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, const DevOp* d_ops,
                   const DenseSegDev* d_dsegs, const double* d_frags, int num_sms, cudaStream_t stream) {
   using A = typename Cplx<Real>::T;
@@ -585,12 +620,12 @@ int launch_tile_t(void* amp, const DevPass& pass, const DevSegment* d_segs, cons
   const size_t smem = sizeof(A) << (pass.L + pass.H);
   prepare_tile_t<Real>();
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<Real>, NT, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<Real, DENSE>, NT, smem);
   if (per_sm < 1) per_sm = 1;
   uint64_t grid = (uint64_t)num_sms * per_sm;
   if (grid > pass.num_tiles) grid = pass.num_tiles;
-  k_tile<Real><<<(unsigned)grid, NT, smem, stream>>>(reinterpret_cast<A*>(amp), pass, d_segs, d_ops, d_dsegs,
-                                                     d_frags);
+  k_tile<Real, DENSE><<<(unsigned)grid, NT, smem, stream>>>(reinterpret_cast<A*>(amp), pass, d_segs, d_ops,
+                                                            d_dsegs, d_frags);
   count_launch();
   return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
 }
@@ -656,12 +691,17 @@ void prepare_tile_launch(int dtype) {
 
 int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment* d_segs,
                      const DevOp* d_ops, const DenseSegDev* d_dsegs, const double* d_frags, int num_sms,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, bool all_dense) {
   if (pass.num_segments < 1 || pass.num_segments > kMaxPassSegs) return MLB_ERR_INVALID_ARG;
-  if (pass.H > 13 - (kLowBitsC128 < 5 ? kLowBitsC128 : 5)) return MLB_ERR_INVALID_ARG;  // row table size
-  if (dtype == MLB_C128)
-    return launch_tile_t<double>(amp, pass, d_segs, d_ops, d_dsegs, d_frags, num_sms, stream);
-  return launch_tile_t<float>(amp, pass, d_segs, d_ops, nullptr, nullptr, num_sms, stream);
+  // row table size: a tile of a state larger than one tile has the dtype's low bits
+  const int TB = dtype == MLB_C128 ? TileCfg<double>::TB : TileCfg<float>::TB;
+  const int LOW = dtype == MLB_C128 ? TileCfg<double>::LOW : TileCfg<float>::LOW;
+  if (pass.L + pass.H > TB || (pass.H > 0 && pass.L != LOW)) return MLB_ERR_INVALID_ARG;
+  if (dtype == MLB_C128) {
+    if (all_dense) return launch_tile_t<double, true>(amp, pass, d_segs, d_ops, d_dsegs, d_frags, num_sms, stream);
+    return launch_tile_t<double, false>(amp, pass, d_segs, d_ops, d_dsegs, d_frags, num_sms, stream);
+  }
+  return launch_tile_t<float, false>(amp, pass, d_segs, d_ops, nullptr, nullptr, num_sms, stream);
 }
 
 }  // namespace mlb

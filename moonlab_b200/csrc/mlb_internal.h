@@ -56,7 +56,10 @@ struct DevSegment {
 };
 
 constexpr int kMaxHigh = 16;
-constexpr int kLowBitsC128 = 3;  // contiguous low qubits of a complex128 tile (planner.h)
+// complex128 tile passes: tiles of 2^12 amplitudes (64 KiB, two CTAs per SM)
+// with 2 contiguous low qubits (64-byte rows) and 10 chosen high ones
+constexpr int kTileBitsC128 = 12;
+constexpr int kLowBitsC128 = 2;  // contiguous low qubits of a complex128 tile (planner.h)
 // A pass's op program is decoded into shared memory; the planner keeps every
 // pass within these sizes.
 constexpr int kMaxPassOps = 160;
@@ -82,20 +85,22 @@ struct DevPass {
 // by group, outside ones by tile): one matrix variant per value of those
 // bits.  Offsets are in 16-byte tile elements, already swizzled (the tile
 // swizzle is linear over GF(2)).
+constexpr int kDenseGroupBits = kTileBitsC128 - 4;   // 256 groups of 16 amplitudes per tile
+constexpr int kDenseColBits = kDenseGroupBits - 3;   // 32 column tiles of 8 groups
 constexpr int kDenseMaxCond = 6;     // conditioning qubits in all (64 variants)
-constexpr int kDenseMaxCondLoc = 5;  // of them tile-local (the top group-index bits; a column-tile pair shares one)
+constexpr int kDenseMaxCondLoc = kDenseColBits - 1;  // of them tile-local (the top group-index bits; a column-tile pair shares one)
 constexpr int kDenseMaxCondOut = 6;  // of them outside the tile
 // doubles per matrix variant: Re U and Im U as 2 x 8 A fragments of 32 lanes
 constexpr int kDenseVarDoubles = 512;
 struct DenseSegDev {
   uint32_t frag_off;   // first double of variant 0 in the fragment pool (kDenseVarDoubles per variant)
-  uint8_t nloc;        // tile-local conditioning qubits: group-index bits 9 - nloc .. 8
+  uint8_t nloc;        // tile-local conditioning qubits: the top nloc group-index bits
   uint8_t nout;        // outside conditioning qubits: global bits obit[0 .. nout)
   uint8_t pad[2];
   uint8_t obit[8];
   uint16_t amp_off[16];  // fragment slot a -> offset
   uint16_t g_lo[8];      // group-index bits 0..2 -> offset
-  uint16_t g_hi[64];     // group-index bits 3..8 -> offset
+  uint16_t g_hi[1 << kDenseColBits];  // group-index bits 3.. -> offset
 };
 // Swizzle of a complex128 tile in shared memory (16-byte elements, 8 per
 // 128-byte row): bits 0..2 (the bank group) xor the fold of all higher bits
@@ -162,9 +167,11 @@ int launch_gram(const void* states, uint64_t dim, int B, double2* d_G, void* d_s
 // Kernel launchers (kernels_*.cu).  All asynchronous on `stream`.
 // d_dsegs / d_frags: the program's dense segments and their matrix fragments
 // (complex128 segments of mode 2; may be null when there are none).
+// all_dense: every segment of the pass is a dense complex128 segment (mode
+// 2); such passes run a kernel that holds only the dense code.
 int launch_tile_pass(int dtype, void* amp, const DevPass& pass, const DevSegment* d_segs,
                      const DevOp* d_ops, const DenseSegDev* d_dsegs, const double* d_frags, int num_sms,
-                     cudaStream_t stream);
+                     cudaStream_t stream, bool all_dense = false);
 // Sets the tile kernel's function attributes on the current device (done
 // lazily by launch_tile_pass; called before a stream capture).
 void prepare_tile_launch(int dtype);
@@ -246,6 +253,6 @@ int prepare_ops(const mlb_gate_t* gates, size_t num_gates, uint32_t n, std::vect
 
 // d_err: device word set non-zero if a tensor-core completion wait ran out.
 int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,
-                      const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream);
+                      const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream, int test_skip_copy = 0);
 
 }  // namespace mlb

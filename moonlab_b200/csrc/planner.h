@@ -19,7 +19,7 @@ inline int popc(uint64_t x) { return __builtin_popcountll(x); }
 struct Geo {
   int TB, RB;
 };
-inline Geo geo(int dtype) { return dtype == MLB_C128 ? Geo{13, 4} : Geo{13, 4}; }  // same tile shape for both dtypes
+inline Geo geo(int dtype) { return dtype == MLB_C128 ? Geo{kTileBitsC128, 4} : Geo{13, 4}; }
 
 // Non-diagonal target qubits of an op (must lie inside a tile) and all the
 // qubits it touches (targets, controls, diagonal keys).
@@ -57,7 +57,7 @@ struct Planner {
   // outside its four register bits) past what one dense 16x16 segment holds,
   // since a segment over the limit runs gate by gate at several times the
   // cost; a segment is padded with conditioning bits first, and a pass's
-  // unused high slots are filled so that every tile has 13 bits
+  // unused high slots are filled so that every tile has all its bits
   bool dense_limits = false;
   std::vector<PlannedPass> passes;
   std::vector<DevSegment> segs;
@@ -366,9 +366,10 @@ struct Planner {
   void plan(const std::vector<mlb_op_t>& ops) {
     std::vector<int> rem(ops.size());
     for (size_t i = 0; i < ops.size(); i++) rem[i] = (int)i;
-    // contiguous low qubits of every tile: complex128 keeps 3 (128-byte rows,
-    // still whole cache lines; more room for the high qubits the ops need:
-    // 49 passes instead of 60 for the 30-qubit depth-40 circuit), complex64 5
+    // contiguous low qubits of every tile: complex128 keeps 2 (64-byte rows,
+    // two 32-byte sectors; more room for the high qubits the ops need: the
+    // 30-qubit depth-40 circuit takes 45 passes of 12-bit tiles, against 55
+    // with 3 low qubits), complex64 5
     const int L = (int)n <= g.TB ? (int)n : (dtype == MLB_C128 ? kLowBitsC128 : 5);
     while (!rem.empty()) {
       uint64_t SH = 0;

@@ -80,3 +80,26 @@ def test_fused_mode_falls_back_to_tile_passes(gpu):
     want = B.port_run_from(n, g[len(g) // 2:], b)
     assert st["dense_blocks"] > 0
     assert np.abs(got - want).max() < 1e-5
+
+
+def test_bounded_wait_reports_timeout_and_the_state_recovers(gpu):
+    """The fused kernel's mbarrier waits are bounded: with CTA 0's first
+    operand-image copy withheld (mlb_test_fused_skip_copy) its waits run out
+    (20 ms each, no copy and no MMA in flight), the synchronize reports
+    MLB_ERR_TIMEOUT, and the same state then reruns the circuit correctly."""
+    from moonlab_b200 import _lib
+    lib = _lib.load()
+    n = 16
+    g = brickwork(n, 6, 0x7AB, zz_every=3)
+    want = B.port_run(n, g)
+    with StateVector(n, "c64") as sv:
+        sv.set_exec_mode("fused")
+        assert lib.mlb_test_fused_skip_copy(sv.handle) == 0
+        sv.run(g)
+        assert lib.mlb_flush(sv.handle) == 0
+        assert lib.mlb_synchronize(sv.handle) == -7  # MLB_ERR_TIMEOUT
+        sv.reset()
+        sv.run(g)
+        got = sv.amplitudes().astype(np.complex128)
+    fid = abs(np.vdot(want, got)) ** 2 / np.vdot(got, got).real
+    assert fid >= 1 - 1e-6

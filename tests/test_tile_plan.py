@@ -19,6 +19,9 @@ OP_1Q, OP_2Q, OP_DIAG1, OP_X, OP_SWAP, OP_ZZ, OP_PHASE = range(7)
 _IDX = {}
 
 
+C128_TILE_BITS = 12  # complex128 tiles: 2 contiguous low qubits + 10 chosen high ones
+
+
 def apply_op(a, n, o):
     """mlb_op_t semantics (moonlab_b200.h) on a numpy state, in place."""
     idx = _IDX.setdefault(n, np.arange(1 << n, dtype=np.uint64))
@@ -105,7 +108,7 @@ def check_structure(n, passes, segs, planned, dtype):
             if s.mode == 1:
                 assert len(ops) == 1 and ops[0].kind == OP_2Q
             if s.mode == 2:
-                assert dtype == _lib.MLB_C128 and L + H == 13 and s.nbits == 4
+                assert dtype == _lib.MLB_C128 and L + H == C128_TILE_BITS and s.nbits == 4
     # the segments cover the execution order once, in order
     flat = [i for b, e in covered for i in range(b, e)]
     assert flat == list(range(len(planned)))
@@ -159,7 +162,7 @@ def test_complex128_segments_all_run_dense(name):
     ops = gates_to_ops(make(), n)
     passes, segs, planned = tile_plan(ops, n, _lib.MLB_C128)
     assert all(s.mode == 2 for s in segs)
-    assert all(p.num_low + p.num_high == 13 for p in passes)  # high slots filled
+    assert all(p.num_low + p.num_high == C128_TILE_BITS for p in passes)  # high slots filled
 
 
 def test_unfused_plan_keeps_every_op():
