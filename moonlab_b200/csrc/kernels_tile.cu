@@ -224,11 +224,7 @@ __device__ __forceinline__ int dense_variant(const DenseSegDev* __restrict__ sg,
 // dense segment (have_pf); nsg / nbase: the next dense segment and its tile,
 // whose first variant this call loads into pf during its last step, so the
 // L2 latency of the fragments overlaps that step and the barrier.
-// PIPE (passes whose segments all run dense): the next step's operands are
-// loaded before this step's DMMAs, so their shared-memory latency overlaps
-// the tensor-core work; the kernel that also holds gate-by-gate segments
-// keeps the loads in the step (its registers are spent on those).
-template <int NT, bool PIPE>
+template <int NT>
 __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const DenseSegDev* __restrict__ sg,
                                               const double* __restrict__ frags, uint64_t tile_base,
                                               bool have_pf, double (&pf)[16],
@@ -248,7 +244,6 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
   const double* fseg = frags + sg->frag_off + lane;
   int cur = -1;
   double ar[8], aj[8];  // fragment (i, s) at index 4 i + s
-  double2 x0[4], x1[4];        // this step's B operands (two column tiles)
   // two column tiles per step: 12 independent accumulator chains per warp
   // cover the DMMA latency; they differ only in bit 0 of j, so they share
   // their conditioning values (the top nloc <= 5 of j's 6 bits)
@@ -274,23 +269,11 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
       }
       cur = var;
     }
-    if (u == 0 || !PIPE) {
+    double2 x0[4], x1[4];  // this step's B operands (two column tiles)
 #pragma unroll
-      for (int t4 = 0; t4 < 4; t4++) {
-        x0[t4] = sm[ghi0 ^ glb ^ boff[t4]];
-        x1[t4] = sm[ghi1 ^ glb ^ boff[t4]];
-      }
-    }
-    // the next step's operands (column tiles j + 2, j + 3: groups no other
-    // step of this segment writes) are loaded before this step's DMMAs
-    double2 y0[4], y1[4];
-    if (PIPE && u + 2 < kPerWarp) {
-      const uint32_t nh0 = sg->g_hi[j + 2], nh1 = sg->g_hi[j + 3];
-#pragma unroll
-      for (int t4 = 0; t4 < 4; t4++) {
-        y0[t4] = sm[nh0 ^ glb ^ boff[t4]];
-        y1[t4] = sm[nh1 ^ glb ^ boff[t4]];
-      }
+    for (int t4 = 0; t4 < 4; t4++) {
+      x0[t4] = sm[ghi0 ^ glb ^ boff[t4]];
+      x1[t4] = sm[ghi1 ^ glb ^ boff[t4]];
     }
     if (u == kPerWarp - 2 && nsg != nullptr) {  // last step: fetch the next segment's first variant
       const double* f = frags + nsg->frag_off + lane +
@@ -334,18 +317,12 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
     sm[ghi1 ^ gld0 ^ doff1] = out(1, 1, 0);
     sm[ghi1 ^ gld1 ^ doff0] = out(1, 0, 1);
     sm[ghi1 ^ gld1 ^ doff1] = out(1, 1, 1);
-    if (PIPE && u + 2 < kPerWarp) {
-#pragma unroll
-      for (int t4 = 0; t4 < 4; t4++) {
-        x0[t4] = y0[t4];
-        x1[t4] = y1[t4];
-      }
-    }
   }
 }
 
 // DENSE (complex128 passes whose segments all run dense): only the dense
-// segment code, pipelined; no op program to decode.
+// segment code, no op program to decode (fewer registers and less shared
+// memory than the kernel that also runs gate-by-gate segments).
 template <typename Real, bool DENSE>
 __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
     k_tile(typename Cplx<Real>::T* __restrict__ amp, const DevPass pass,
@@ -476,8 +453,8 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
             nsg = dsegs + ssegs[0].dense;
             nbase = pdep64(tile + gridDim.x, pass.tile_free_mask);
           }
-          dense_segment<NT, DENSE>(reinterpret_cast<double2*>(sm), dsegs + seg.dense, frags, tile_base, have_pf,
-                                   pf, nsg, nbase);
+          dense_segment<NT>(reinterpret_cast<double2*>(sm), dsegs + seg.dense, frags, tile_base, have_pf, pf,
+                            nsg, nbase);
           have_pf = nsg != nullptr;
           __syncthreads();
           continue;
