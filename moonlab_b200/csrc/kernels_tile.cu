@@ -247,10 +247,13 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
   // two column tiles per step: 12 independent accumulator chains per warp
   // cover the DMMA latency; they differ only in bit 0 of j, so they share
   // their conditioning values (the top nloc <= 5 of j's 6 bits)
+  // this warp's column-tile offsets, one per lane, passed along by shuffles
+  // (no table read in the step's dependency chain)
+  const uint32_t my_ghi = sg->g_hi[kPerWarp * warp + (lane % kPerWarp)];
 #pragma unroll 1
   for (int u = 0; u < kPerWarp; u += 2) {
     const int j = kPerWarp * warp + u;  // column tiles j, j + 1: groups 8 j .. 8 j + 15
-    const uint32_t ghi0 = sg->g_hi[j], ghi1 = sg->g_hi[j + 1];
+    const uint32_t ghi0 = __shfl_sync(0xffffffffu, my_ghi, u), ghi1 = __shfl_sync(0xffffffffu, my_ghi, u + 1);
     const int var = (nloc ? (j >> (kDenseColBits - nloc)) : 0) | (int)(vout << nloc);
     if (var != cur) {  // warp-uniform
       if (u == 0 && have_pf) {
@@ -342,6 +345,8 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   __shared__ uint8_t ton[kProg];
   __shared__ uint8_t tkey[kProg];
   __shared__ DevSegment ssegs[kMaxPassSegs];
+  // dense-only passes: the segments' offset tables in shared memory
+  __shared__ DenseSegDev sdseg[DENSE ? kMaxPassSegs : 1];
 
   const int L = pass.L, H = pass.H;
   const uint32_t tile_amps = 1u << (L + H);
@@ -362,6 +367,7 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
     sg.op_begin -= op0;
     sg.op_end -= op0;
     ssegs[s] = sg;
+    if constexpr (DENSE) sdseg[s] = dsegs[sg.dense];
   }
   for (int o = threadIdx.x; o < (DENSE ? 0 : nops); o += NT) {
     const DevOp& d = ops[op0 + o];
@@ -448,13 +454,13 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
           const DenseSegDev* nsg = nullptr;
           uint64_t nbase = tile_base;
           if (s + 1 < nseg) {
-            if (ssegs[s + 1].mode == 2) nsg = dsegs + ssegs[s + 1].dense;
+            if (ssegs[s + 1].mode == 2) nsg = DENSE ? sdseg + s + 1 : dsegs + ssegs[s + 1].dense;
           } else if (tile + gridDim.x < pass.num_tiles && ssegs[0].mode == 2) {
-            nsg = dsegs + ssegs[0].dense;
+            nsg = DENSE ? sdseg : dsegs + ssegs[0].dense;
             nbase = pdep64(tile + gridDim.x, pass.tile_free_mask);
           }
-          dense_segment<NT>(reinterpret_cast<double2*>(sm), dsegs + seg.dense, frags, tile_base, have_pf, pf,
-                            nsg, nbase);
+          dense_segment<NT>(reinterpret_cast<double2*>(sm), DENSE ? sdseg + s : dsegs + seg.dense, frags, tile_base,
+                            have_pf, pf, nsg, nbase);
           have_pf = nsg != nullptr;
           __syncthreads();
           continue;
