@@ -212,23 +212,9 @@ __device__ __forceinline__ void dmma_f64(double& d0, double& d1, double a, doubl
 // operands are whole input slots 4 s + c of group r (re for t1, im for t2,
 // their sum for t3) and its D results whole output slots r and 8 + r of
 // groups 2 c and 2 c + 1.
-// Matrix variant of column tile j of a dense segment in the tile at tile_base.
-__device__ __forceinline__ int dense_variant(const DenseSegDev* __restrict__ sg, uint64_t tile_base, int j) {
-  const int nloc = sg->nloc, nout = sg->nout;
-  uint32_t vout = 0;
-  for (int k = 0; k < nout; k++) vout |= (uint32_t)((tile_base >> sg->obit[k]) & 1ull) << k;
-  return (nloc ? (j >> (kDenseColBits - nloc)) : 0) | (int)(vout << nloc);
-}
-
-// pf: this warp's first matrix variant of the segment, loaded by the previous
-// dense segment (have_pf); nsg / nbase: the next dense segment and its tile,
-// whose first variant this call loads into pf during its last step, so the
-// L2 latency of the fragments overlaps that step and the barrier.
 template <int NT>
 __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const DenseSegDev* __restrict__ sg,
-                                              const double* __restrict__ frags, uint64_t tile_base,
-                                              bool have_pf, double (&pf)[16],
-                                              const DenseSegDev* __restrict__ nsg, uint64_t nbase) {
+                                              const double* __restrict__ frags, uint64_t tile_base) {
   constexpr int kWarps = NT / 32, kPerWarp = (1 << kDenseColBits) / kWarps;  // column tiles of 8 groups
   // warp w takes column tiles kPerWarp w .. + kPerWarp - 1: their conditioning
   // values (the top group-index bits) rarely change within a warp
@@ -256,19 +242,11 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
     const uint32_t ghi0 = __shfl_sync(0xffffffffu, my_ghi, u), ghi1 = __shfl_sync(0xffffffffu, my_ghi, u + 1);
     const int var = (nloc ? (j >> (kDenseColBits - nloc)) : 0) | (int)(vout << nloc);
     if (var != cur) {  // warp-uniform
-      if (u == 0 && have_pf) {
+      const double* f = fseg + (size_t)var * kDenseVarDoubles;
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-          ar[k] = pf[k];
-          aj[k] = pf[8 + k];
-        }
-      } else {
-        const double* f = fseg + (size_t)var * kDenseVarDoubles;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          ar[k] = __ldg(f + 32 * k);
-          aj[k] = __ldg(f + 32 * (8 + k));
-        }
+      for (int k = 0; k < 8; k++) {
+        ar[k] = __ldg(f + 32 * k);
+        aj[k] = __ldg(f + 32 * (8 + k));
       }
       cur = var;
     }
@@ -277,12 +255,6 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
     for (int t4 = 0; t4 < 4; t4++) {
       x0[t4] = sm[ghi0 ^ glb ^ boff[t4]];
       x1[t4] = sm[ghi1 ^ glb ^ boff[t4]];
-    }
-    if (u == kPerWarp - 2 && nsg != nullptr) {  // last step: fetch the next segment's first variant
-      const double* f = frags + nsg->frag_off + lane +
-                        (size_t)dense_variant(nsg, nbase, kPerWarp * warp) * kDenseVarDoubles;
-#pragma unroll
-      for (int k = 0; k < 16; k++) pf[k] = __ldg(f + 32 * k);
     }
     // [column tile][product][m-tile][column]
     double t[2][3][2][2];
@@ -409,8 +381,6 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   const bool full = tile_amps == (1u << TB);
   const uint32_t sm_base = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
   bool prefetched = false;
-  double pf[16];  // next dense segment's first matrix variant (dense_segment)
-  bool have_pf = false;
   for (uint64_t tile = blockIdx.x; tile < pass.num_tiles; tile += gridDim.x) {
     const uint64_t tile_base = pdep64(tile, pass.tile_free_mask);
     // tile-constant op predicates and keys
@@ -449,26 +419,11 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
       const DevSegment& seg = ssegs[s];
       if constexpr (sizeof(Real) == 8) {
         if (seg.mode == 2) {
-          // the next dense segment: this tile's next one, or the first of the
-          // CTA's next tile
-          const DenseSegDev* nsg = nullptr;
-          uint64_t nbase = tile_base;
-          if (s + 1 < nseg) {
-            if (ssegs[s + 1].mode == 2) nsg = DENSE ? sdseg + s + 1 : dsegs + ssegs[s + 1].dense;
-          } else if (tile + gridDim.x < pass.num_tiles && ssegs[0].mode == 2) {
-            nsg = DENSE ? sdseg : dsegs + ssegs[0].dense;
-            nbase = pdep64(tile + gridDim.x, pass.tile_free_mask);
-          }
-          dense_segment<NT>(reinterpret_cast<double2*>(sm), DENSE ? sdseg + s : dsegs + seg.dense, frags, tile_base,
-                            have_pf, pf, nsg, nbase);
-          have_pf = nsg != nullptr;
+          dense_segment<NT>(reinterpret_cast<double2*>(sm), DENSE ? sdseg + s : dsegs + seg.dense, frags,
+                            tile_base);
           __syncthreads();
           continue;
         }
-        // pf is not carried across other segments (keeps it out of their registers)
-        have_pf = false;
-#pragma unroll
-        for (int k = 0; k < 16; k++) pf[k] = 0.0;
       }
       if constexpr (!DENSE) {
       if (seg.mode == 1) {

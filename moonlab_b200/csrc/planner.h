@@ -4,6 +4,7 @@
 #pragma once
 
 #include <algorithm>
+#include <iterator>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -59,6 +60,10 @@ struct Planner {
   // cost; a segment is padded with conditioning bits first, and a pass's
   // unused high slots are filled so that every tile has all its bits
   bool dense_limits = false;
+  // with dense_limits: a pass's last register segment of at most this many
+  // ops goes back to the remaining ops (it would cost a whole dense segment;
+  // the next pass usually takes it into one of its segments)
+  int defer_tail = 6;
   std::vector<PlannedPass> passes;
   std::vector<DevSegment> segs;
   std::vector<DevOp> dops;
@@ -398,6 +403,26 @@ struct Planner {
         }
       }
       lower_pass(ops, taken, L, SH);
+      if (dense_limits && defer_tail > 0 && (int)n > g.TB) {
+        PlannedPass& pp = passes.back();
+        const DevSegment& last = segs[pp.seg_end - 1];
+        const int nlast = last.op_end - last.op_begin;
+        if (pp.pass.num_segments >= 2 && last.mode == 0 && nlast <= defer_tail) {
+          // the last segment's ops were scheduled after every other op of the
+          // pass (they depend on or commute with all of them), so running
+          // them after the whole pass keeps the circuit
+          std::vector<int> back(dop_src.begin() + last.op_begin, dop_src.end());
+          std::sort(back.begin(), back.end());
+          dops.resize(last.op_begin);
+          dop_src.resize(last.op_begin);
+          segs.pop_back();
+          pp.seg_end--;
+          pp.pass.num_segments--;
+          std::vector<int> kept;
+          std::set_difference(taken.begin(), taken.end(), back.begin(), back.end(), std::back_inserter(kept));
+          taken.swap(kept);
+        }
+      }
       // remove taken (both lists ascending)
       std::vector<int> next;
       next.reserve(rem.size() - taken.size());

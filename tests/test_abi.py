@@ -110,9 +110,11 @@ def test_planner_groups_the_brickwork_workloads():
     st = plan(g2, 30)
     assert st.passes <= 80                         # vs 4470 sweeps gate by gate
     assert st.bytes_moved == st.passes * 2 * 16 * (1 << 30)
-    assert st.passes <= 55                         # c128: 3 contiguous low qubits per tile
-    # c128: every register segment runs as a dense matrix (segments close
-    # before their conditioning qubits outgrow one; full 13-bit tiles)
+    # c128: 12-bit tiles (2 contiguous low qubits), a pass's short trailing
+    # segment deferred to the next pass: a few more passes, fewer dense segments
+    assert st.passes <= 60 and st.segments <= 160
+    # every register segment runs as a dense matrix (segments close before
+    # their conditioning qubits outgrow one; full tiles)
     assert st.dense_blocks == st.segments
     for n in (16, 22, 26):
         st = plan(brickwork(n, 40, 0xC2, zz_every=4), n)
