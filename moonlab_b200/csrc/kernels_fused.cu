@@ -25,8 +25,8 @@
 // their 32 accumulator lanes back (tcgen05.ld 32x32b) into the FP32 tile.
 //
 // Occupancy: a CTA of 8 warps (warp w owns tensor-memory lane quadrant w & 3
-// of half w >> 2, one tile row per thread) holds one tile buffer, the
-// block's operand image and 256 TMEM columns, so two CTAs share an SM: one
+// of half w >> 2, one tile row per thread) holds one tile buffer, two
+// operand images (110 KiB of shared memory) and 256 TMEM columns, so two CTAs share an SM: one
 // CTA's MMA waits and tile loads (16-byte async copies, cp.async) overlap
 // the other's operand conversion and readback.  A tile's loads are issued
 // from the previous tile's store loop, into the slots just stored, so they
@@ -36,8 +36,10 @@
 // every ~70 cycles, so one issuer alone would leave the tensor core half idle
 // at N = 64.  MMA descriptors are precomputed (the per-MMA part is a
 // constant add).  Each block's operand image comes by one bulk copy
-// completing on its own mbarrier, requested as soon as both halves' MMAs
-// have completed.
+// completing on its buffer's mbarrier; there are two image buffers, and the
+// image two applications ahead is requested as soon as both halves' MMAs of
+// the current one have completed, so a copy has a whole block's conversion,
+// MMAs and readback to land.
 //
 // Waits are bounded: if one runs out the kernel sets *err, waits once more
 // (bounded) for what it issued, frees its tensor memory and returns.
@@ -56,20 +58,27 @@ constexpr int kFThreads = 256;       // 8 warps: warp w owns TMEM lane quadrant 
 constexpr int kTileAmps = 1 << 13;
 constexpr int kPairsPerThread = kTileAmps / 2 / kFThreads;  // 16
 // shared-memory layout (bytes from a 1024-byte aligned base); two CTAs per SM
-constexpr uint32_t kBHi = 0;          // 64 rows x 128 B, then lo
+constexpr uint32_t kBHi = 0;          // operand image buffer 0: 64 rows x 128 B, then lo
 constexpr uint32_t kBLo = 8192;
-constexpr uint32_t kTile0 = 16384;    // one tile buffer of 2^13 float2 (64 KiB)
-constexpr uint32_t kMbarMma = 81920;  // two: one per 128-row half
-constexpr uint32_t kMbarB = 81936;
-constexpr uint32_t kTmemSlot = 81944;
-constexpr uint32_t kFlag = 81948;
+constexpr uint32_t kBImg = 16384;     // buffer 1 at kBImg (two images in flight)
+constexpr uint32_t kTile0 = 32768;    // one tile buffer of 2^13 float2 (64 KiB)
+constexpr uint32_t kMbarMma = 98304;  // two: one per 128-row half
+constexpr uint32_t kMbarB = 98320;    // two: one per image buffer
+constexpr uint32_t kTmemSlot = 98336;
+constexpr uint32_t kFlag = 98340;
+constexpr uint32_t kIssued = 98344;   // two uint32: image copies issued into each buffer
 constexpr int kMaxBlocks = 64;        // blocks per pass (the planner splits longer passes)
-constexpr uint32_t kColTab = 81952;   // per block: 32 swizzled column offsets (uint32)
+constexpr uint32_t kColTab = 98352;   // per block: 32 swizzled column offsets (uint32)
 constexpr uint32_t kRowTab = kColTab + kMaxBlocks * 128;  // per block: 2 x 16 swizzled row-nibble offsets (uint16)
 constexpr uint32_t kHiDep = kRowTab + kMaxBlocks * 64;    // 16 x uint64: global offsets of tile bits 9..12
 constexpr uint32_t kImgTab = kHiDep + kPairsPerThread * 8;  // per block: operand image index (uint32)
-constexpr uint32_t kSmemUsed = kImgTab + kMaxBlocks * 4;
+constexpr int kTbNibbles = 6;         // tile index bits (<= 34 - 13) in nibbles
+constexpr uint32_t kTbTab = kImgTab + kMaxBlocks * 4;  // 6 x 16 uint64: tile-index nibble -> global bits
+constexpr uint32_t kSmemUsed = kTbTab + kTbNibbles * 16 * 8;
 constexpr uint32_t kSmemBytes = kSmemUsed + 1024;  // alignment slack
+static_assert(kTile0 >= 2 * kBImg && kMbarMma == kTile0 + 65536 && kColTab >= kIssued + 8, "layout overlap");
+static_assert(kColTab % 16 == 0 && kHiDep % 8 == 0 && kTbTab % 8 == 0, "table alignment");
+static_assert(2 * (kSmemBytes + 1024) <= 228 * 1024, "two CTAs per SM (1 KiB reserved per CTA)");
 constexpr uint32_t kTmemCols = 256;  // D: columns 0..127 (64 per half); A: 128..255
 constexpr uint32_t kACol = 128;      // A of half h: hi at kACol + 64 h, lo at kACol + 64 h + 32
 constexpr long long kWaitLimit = 1ll << 24;       // try_wait rounds before giving up (a backstop)
@@ -198,15 +207,13 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
-__device__ __forceinline__ uint64_t tile_base(uint64_t t, uint64_t tmask) {
-  uint64_t gbase = 0, v = t, m = tmask;
-  while (v && m) {
-    const uint64_t low = m & (~m + 1);
-    if (v & 1ull) gbase |= low;
-    v >>= 1;
-    m &= m - 1;
-  }
-  return gbase;
+// Global bits of tile t: the bits of t placed, in order, at the set bits of
+// tmask (the qubits outside the tile), by a 16-entry table per nibble of t.
+__device__ __forceinline__ uint64_t tile_base(uint64_t t, const uint64_t* tbtab) {
+  uint64_t g = 0;
+#pragma unroll
+  for (int k = 0; k < kTbNibbles; k++) g |= tbtab[16 * k + ((t >> (4 * k)) & 15u)];
+  return g;
 }
 
 // Amplitude pair (e, e+1) of a tile -> its global index.
@@ -227,12 +234,17 @@ __global__ void __launch_bounds__(kFThreads, 2)
             const uint8_t* __restrict__ images, int* __restrict__ err, int test_skip_copy) {
   const uint64_t wait_ns = test_skip_copy ? kTestWaitLimitNs : kWaitLimitNs;
   extern __shared__ uint8_t smraw[];
-  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
+  // 1024-byte alignment by pointer arithmetic on the shared array (not
+  // through an integer cast), so every access below stays a shared-memory
+  // access with 32-bit addressing instead of a generic one
+  uint8_t* sm = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
   const uint32_t sbase = smem_u32(sm);
   volatile int* flag = reinterpret_cast<volatile int*>(sm + kFlag);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t half = (uint32_t)warp >> 2, qd = (uint32_t)warp & 3u;  // row m = tid = 128 half + 32 qd + lane
-  const uint32_t bar_mma = sbase + kMbarMma, bar_b = sbase + kMbarB;  // bar_mma + 8 h: half h
+  // bar_mma + 8 h: MMAs of half h done; bar_b + 8 j: operand image in buffer j landed
+  const uint32_t bar_mma = sbase + kMbarMma, bar_b = sbase + kMbarB;
+  volatile uint32_t* issued = reinterpret_cast<volatile uint32_t*>(sm + kIssued);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(sbase + kTmemSlot),
@@ -243,6 +255,9 @@ __global__ void __launch_bounds__(kFThreads, 2)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_mma), "r"(1));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_mma + 8), "r"(1));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_b), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar_b + 8), "r"(1));
+    issued[0] = 0;
+    issued[1] = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     *flag = 0;
   }
@@ -263,15 +278,26 @@ __global__ void __launch_bounds__(kFThreads, 2)
   }
   if (tid < kPairsPerThread)
     reinterpret_cast<uint64_t*>(sm + kHiDep)[tid] = tile_global(0, (uint32_t)tid * 2u * kFThreads, pass);
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTmemSlot);
-
   uint64_t hmask = (1ull << pass.num_low) - 1ull;
 #pragma unroll
   for (int i = 0; i < 12; i++)
     if (i < (int)pass.num_high) hmask |= 1ull << pass.hbits[i];
-  const uint64_t tmask = ~hmask;
+  uint64_t* tbtab = reinterpret_cast<uint64_t*>(sm + kTbTab);
+  if (tid < kTbNibbles * 16) {  // entry (k, v): bits of v at set bits 4k .. 4k+3 of ~hmask
+    const int k = tid >> 4;
+    const uint32_t v = (uint32_t)tid & 15u;
+    uint64_t m = ~hmask, g = 0;
+    for (int j = 0; j < 4 * k && m; j++) m &= m - 1;
+    for (int i = 0; i < 4 && m; i++) {
+      if (v >> i & 1u) g |= m & (~m + 1);
+      m &= m - 1;
+    }
+    tbtab[tid] = g;
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kTmemSlot);
+
 
   // Tile-local index e of this thread's i-th amplitude pair: e = 512 i + 2 tid.
   // Its global offset is linear in e over disjoint bits, so it splits into
@@ -288,17 +314,29 @@ __global__ void __launch_bounds__(kFThreads, 2)
   // shared window is below 256 KiB, so the field does not carry)
   const uint64_t desc_b = sdesc(sbase + kBHi);
 
-  uint32_t ph_mma = 0, ph_b = 0;
+  // Block applications s = 0, 1, ... of this CTA (tile by tile, block by
+  // block) take operand buffer s & 1; application s + 2's image is requested
+  // as soon as application s's MMAs have completed.
+  uint32_t ph_mma = 0, s = 0;
   bool bad = false;
-  if (tid == 0 && (uint64_t)blockIdx.x < pass.num_tiles && !(test_skip_copy && blockIdx.x == 0))
-    bulk_load(sbase + kBHi, images + (size_t)imgtab[0] * 16384, 16384, bar_b);
+  if (tid == 0) {
+    const uint32_t nb = pass.num_blocks;
+    if ((uint64_t)blockIdx.x < pass.num_tiles && !(test_skip_copy && blockIdx.x == 0)) {
+      issued[0] = 1;
+      bulk_load(sbase + kBHi, images + (size_t)imgtab[0] * 16384, 16384, bar_b);
+    }
+    if ((uint64_t)blockIdx.x + (nb > 1 ? 0ull : (uint64_t)gridDim.x) < pass.num_tiles) {
+      issued[1] = 1;
+      bulk_load(sbase + kBImg, images + (size_t)imgtab[nb > 1 ? 1 : 0] * 16384, 16384, bar_b + 8);
+    }
+  }
   float2* tile = reinterpret_cast<float2*>(sm + kTile0);
   // A tile's loads are issued by the previous tile's store loop (each thread
   // refills the 16-byte slots it has just stored), except for the first tile.
   bool prefetched = false;
   for (uint64_t t = blockIdx.x; t < pass.num_tiles && !bad; t += gridDim.x) {
     if (!prefetched) {
-      const uint64_t gb = tile_base(t, tmask) | my_off;
+      const uint64_t gb = tile_base(t, tbtab) | my_off;
       const uint32_t dst0 = sbase + kTile0;
 #pragma unroll 8
       for (int i = 0; i < kPairsPerThread; i++)
@@ -370,7 +408,8 @@ __global__ void __launch_bounds__(kFThreads, 2)
       if (half == 0) asm volatile("bar.sync 1, 128;\n" ::: "memory");
       else asm volatile("bar.sync 2, 128;\n" ::: "memory");
       if (tid == 0 || tid == 160) {
-        if (mbar_wait_bounded(bar_b, ph_b, wait_ns)) {  // operand image landed
+        const uint32_t buf = s & 1u;
+        if (mbar_wait_bounded(bar_b + 8u * buf, (s >> 1) & 1u, wait_ns)) {  // operand image landed
           asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
           const uint32_t a_h = tmem + kACol + half * 64u, d_h = tmem + half * 64u;
 #pragma unroll
@@ -378,7 +417,8 @@ __global__ void __launch_bounds__(kFThreads, 2)
 #pragma unroll
             for (int kk = 0; kk < 4; kk++)
               mma_bf16_ts(d_h, a_h + (kc == 1 ? 32u : 0u) + kk * 8u,
-                          desc_b + (uint64_t)(((kc == 2 ? kBLo : kBHi) + kk * 32u) >> 4), (kc | kk) != 0 ? 1u : 0u);
+                          desc_b + (uint64_t)((buf * kBImg + (kc == 2 ? kBLo : kBHi) + kk * 32u) >> 4),
+                          (kc | kk) != 0 ? 1u : 0u);
           }
           asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                            bar_mma + 8u * half)
@@ -396,10 +436,13 @@ __global__ void __launch_bounds__(kFThreads, 2)
           ok = mbar_wait_bounded(bar_mma + 8u * half, ph_mma, wait_ns) ? 1 : 0;
           if (ok && warp == 5) ok = mbar_wait_bounded(bar_mma, ph_mma, wait_ns) ? 1 : 0;  // and half 0
           if (!ok) atomicOr((int*)flag, 2);
-          if (ok && warp == 5) {
-            const bool more = b + 1 < pass.num_blocks || t + gridDim.x < pass.num_tiles;
-            const uint32_t nb = b + 1 < pass.num_blocks ? b + 1 : 0;
-            if (more) bulk_load(sbase + kBHi, images + (size_t)imgtab[nb] * 16384, 16384, bar_b);
+          if (ok && warp == 5) {  // buffer s & 1 is free: application s + 2's image into it
+            const uint32_t r = b + 2u, adv = r / pass.num_blocks, buf = s & 1u;
+            if (t + (uint64_t)adv * gridDim.x < pass.num_tiles) {
+              issued[buf] = issued[buf] + 1u;
+              bulk_load(sbase + buf * kBImg, images + (size_t)imgtab[r % pass.num_blocks] * 16384, 16384,
+                        bar_b + 8u * buf);
+            }
           }
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -436,7 +479,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
         bad = true;
         break;
       }
-      ph_b ^= 1u;
+      s++;
       ph_mma ^= 1u;
     }
     if (bad) break;
@@ -444,10 +487,10 @@ __global__ void __launch_bounds__(kFThreads, 2)
     // store, and the next tile's loads into the slots just read (this
     // thread's own slots, read before: no barrier needed in between)
     {
-      const uint64_t gb = tile_base(t, tmask) | my_off;
+      const uint64_t gb = tile_base(t, tbtab) | my_off;
       const uint64_t next = t + gridDim.x;
       prefetched = next < pass.num_tiles;
-      const uint64_t ngb = prefetched ? (tile_base(next, tmask) | my_off) : 0;
+      const uint64_t ngb = prefetched ? (tile_base(next, tbtab) | my_off) : 0;
       const uint32_t dst0 = sbase + kTile0;
 #pragma unroll 8
       for (int i = 0; i < kPairsPerThread; i++) {
@@ -463,10 +506,12 @@ __global__ void __launch_bounds__(kFThreads, 2)
 
   // leave no async copy or MMA in flight
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  if (bad && tid == 0) {  // flag bit 1: an operand copy may be pending
+  if (bad && tid == 0) {
     atomicExch(err, 1);
-    const int f = *flag;
-    if (f & 1) mbar_wait_bounded(bar_b, ph_b, wait_ns);
+    // the last image copy issued into each buffer may be pending (at most one
+    // per buffer: a buffer is refilled only after its previous image was used)
+    for (uint32_t j = 0; j < 2; j++)
+      if (issued[j]) mbar_wait_bounded(bar_b + 8u * j, (issued[j] - 1u) & 1u, wait_ns);
     // either half's MMAs may be in flight (the halves have separate issuers)
     mbar_wait_bounded(bar_mma, ph_mma, wait_ns);
     mbar_wait_bounded(bar_mma + 8, ph_mma, wait_ns);
@@ -481,8 +526,8 @@ __global__ void __launch_bounds__(kFThreads, 2)
 
 int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,
                       const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream, int test_skip_copy) {
-  if (n < 13 || pass.num_blocks == 0 || pass.num_blocks > (uint32_t)kMaxBlocks ||
-      pass.num_low < 1 || pass.num_low + pass.num_high != 13)
+  if (n < 13 || n > 13 + 4 * kTbNibbles || pass.num_blocks == 0 || pass.num_blocks > (uint32_t)kMaxBlocks ||
+      pass.num_low < 1 || pass.num_low + pass.num_high != 13 || pass.num_tiles != 1ull << (n - 13))
     return MLB_ERR_INVALID_ARG;
   static std::atomic<uint64_t> attr_set_mask{0};
   int dev = 0;
