@@ -2,10 +2,11 @@
 //
 // One pass reads the whole state once and writes it once, applying a run of
 // gates in between.  A tile is 2^(L+H) amplitudes: L contiguous low qubits
-// (L=5: 512-byte runs for complex128, 256 bytes for complex64, so global
-// loads and stores are fully coalesced 16/8-byte accesses) times the 2^H
-// combinations of H chosen high qubits.  Tiles are enumerated over the
-// remaining n-L-H qubits by a persistent grid sized to the SM count.
+// (complex128: L = 2, 64-byte rows, 12-bit tiles of 64 KiB; complex64: L = 5,
+// 256-byte rows, 13-bit tiles of 64 KiB; global loads and stores are whole
+// 16/8-byte accesses in full rows) times the 2^H combinations of H chosen
+// high qubits.  Tiles are enumerated over the remaining n-L-H qubits by a
+// persistent grid sized to the SM count.
 //
 // Inside a tile the ops are grouped into segments: consecutive ops whose
 // non-diagonal targets span at most R local bits.  For a segment each
@@ -21,13 +22,14 @@
 // moves the bank group; see tile_swz16).
 //
 // complex128 segments that the host multiplied into one 16x16 complex matrix
-// (dense.h; mode 2) run on the FP64 tensor cores instead: the tile's 512
-// groups of 16 amplitudes are the columns of a 16 x 512 complex block, each
-// warp takes 8 groups at a time (an n = 8 column tile), loads them as the B
-// fragments of 4 k-steps (four 16-byte loads per lane), runs 3 real products
-// x 2 m-tiles x 4 k-steps = 24 mma.sync m8n8k4 f64 (Gauss's three-product
-// complex multiplication) with the matrix fragments in registers and stores
-// the results back in place (four 16-byte stores per lane).  Gate by gate, a
+// (dense.h; mode 2) run on the FP64 tensor cores instead: the tile's 256
+// groups of 16 amplitudes are the columns of a 16 x 256 complex block, each
+// warp takes two column tiles of 8 groups at a time, loads them as the B
+// fragments of 4 k-steps (four 16-byte loads per lane per column tile), runs
+// 3 real products x 2 m-tiles x 4 k-steps = 24 mma.sync m8n8k4 f64 per column
+// tile (Gauss's three-product complex multiplication) with the matrix
+// fragments in registers and stores the results back in place (four 16-byte
+// stores per lane per column tile).  Gate by gate, a
 // segment's ~12 ops cost about as many FP64 multiply-adds as the dense
 // product (48 per amplitude) but spend two thirds of their instruction issue
 // on addressing, dispatch and register moves; one DMMA is 256 of them.
@@ -52,8 +54,11 @@ template <> struct TileCfg<float> {   // complex64: 2^13 amps = 64 KiB per CTA
 };
 // GPT: register groups per thread per segment, interleaved for ILP.  LOW:
 // contiguous low qubits of a tile of a state larger than one tile (rows).
-// Two complex128 CTAs per SM run independent tile sequences, so one CTA's
-// loads and stores overlap the other's tensor-core work.
+// complex128 CTAs on one SM run independent tile sequences, so one CTA's
+// loads and stores overlap the others' tensor-core work: two per SM in
+// general, three in dense-only passes (a CTA of 4 warps keeps the FP64
+// tensor pipe busy only together with others: with two per SM, the pipe
+// starves while one of them is in its memory phase).
 
 template <typename Real>
 __device__ __forceinline__ uint32_t swz(uint32_t e) {
@@ -299,7 +304,7 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
 // segment code, no op program to decode (fewer registers and less shared
 // memory than the kernel that also runs gate-by-gate segments).
 template <typename Real, bool DENSE>
-__global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
+__global__ void __launch_bounds__(TileCfg<Real>::NT, DENSE ? 3 : TileCfg<Real>::MINB)
     k_tile(typename Cplx<Real>::T* __restrict__ amp, const DevPass pass,
            const DevSegment* __restrict__ segs, const DevOp* __restrict__ ops,
            const DenseSegDev* __restrict__ dsegs, const double* __restrict__ frags) {
@@ -316,9 +321,13 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   __shared__ A smat[kProg][4];
   __shared__ uint8_t ton[kProg];
   __shared__ uint8_t tkey[kProg];
-  __shared__ DevSegment ssegs[kMaxPassSegs];
-  // dense-only passes: the segments' offset tables in shared memory
-  __shared__ DenseSegDev sdseg[DENSE ? kMaxPassSegs : 1];
+  __shared__ DevSegment ssegs[DENSE ? 1 : kMaxPassSegs];
+  // dense-only passes: two staging slots for the segments' offset tables
+  // (application q reads slot q & 1 while application q + 1's is staged)
+  // and the segments' dense indices; small enough for three CTAs per SM
+  __shared__ DenseSegDev sdseg[DENSE ? 2 : 1];
+  __shared__ uint16_t didx[DENSE ? kMaxPassSegs : 1];
+  static_assert(sizeof(DenseSegDev) == 128, "staged as 32 words");
 
   const int L = pass.L, H = pass.H;
   const uint32_t tile_amps = 1u << (L + H);
@@ -334,12 +343,18 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
       if (k < H && (r >> k & 1u)) off |= 1ull << pass.high[k];
     rowoff[r] = off;
   }
-  for (int s = threadIdx.x; s < nseg; s += NT) {
-    DevSegment sg = segs[s];
-    sg.op_begin -= op0;
-    sg.op_end -= op0;
-    ssegs[s] = sg;
-    if constexpr (DENSE) sdseg[s] = dsegs[sg.dense];
+  if constexpr (DENSE) {
+    for (int s = threadIdx.x; s < nseg; s += NT) didx[s] = (uint16_t)segs[s].dense;
+    if (threadIdx.x < 32)
+      reinterpret_cast<uint32_t*>(sdseg)[threadIdx.x] =
+          reinterpret_cast<const uint32_t*>(dsegs + segs[0].dense)[threadIdx.x];
+  } else {
+    for (int s = threadIdx.x; s < nseg; s += NT) {
+      DevSegment sg = segs[s];
+      sg.op_begin -= op0;
+      sg.op_end -= op0;
+      ssegs[s] = sg;
+    }
   }
   for (int o = threadIdx.x; o < (DENSE ? 0 : nops); o += NT) {
     const DevOp& d = ops[op0 + o];
@@ -381,6 +396,7 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
   const bool full = tile_amps == (1u << TB);
   const uint32_t sm_base = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
   bool prefetched = false;
+  uint32_t dq = 0;  // dense-only passes: segment applications so far (staging slot parity)
   for (uint64_t tile = blockIdx.x; tile < pass.num_tiles; tile += gridDim.x) {
     const uint64_t tile_base = pdep64(tile, pass.tile_free_mask);
     // tile-constant op predicates and keys
@@ -416,11 +432,22 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, TileCfg<Real>::MINB)
     __syncthreads();
 
     for (int s = 0; s < nseg; s++) {
+      if constexpr (DENSE) {
+        // stage the next application's table (the next segment, or segment 0
+        // of the next tile) into the other slot; the barrier publishes it
+        const int sn = s + 1 < nseg ? s + 1 : 0;
+        uint32_t w = 0;
+        if (threadIdx.x < 32) w = reinterpret_cast<const uint32_t*>(dsegs + didx[sn])[threadIdx.x];
+        dense_segment<NT>(reinterpret_cast<double2*>(sm), sdseg + (dq & 1u), frags, tile_base);
+        if (threadIdx.x < 32) reinterpret_cast<uint32_t*>(sdseg + ((dq + 1u) & 1u))[threadIdx.x] = w;
+        dq++;
+        __syncthreads();
+        continue;
+      }
       const DevSegment& seg = ssegs[s];
       if constexpr (sizeof(Real) == 8) {
         if (seg.mode == 2) {
-          dense_segment<NT>(reinterpret_cast<double2*>(sm), DENSE ? sdseg + s : dsegs + seg.dense, frags,
-                            tile_base);
+          dense_segment<NT>(reinterpret_cast<double2*>(sm), dsegs + seg.dense, frags, tile_base);
           __syncthreads();
           continue;
         }
