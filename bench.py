@@ -38,7 +38,16 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "30q circuit time & HBM GB/s (fused c64 vs plain c128); circuits/s, p99 at load"
-WORKLOAD = "30q depth-40 brickwork RX/RY/RZ+CNOT, ZZ(theta) layer every 4 layers (4470 gates)"
+def workload(n: int, depth: int, gates: int) -> str:
+    """The circuit workload's name ("30q depth-40 ... (4470 gates)" by default)."""
+    return f"{n}q depth-{depth} brickwork RX/RY/RZ+CNOT, ZZ(theta) layer every 4 layers ({gates} gates)"
+
+
+def l2_note(n: int) -> str:
+    """Whether a complex128 state of n qubits is larger than the 126 MB L2."""
+    size = 16 << n
+    human = f"{size >> 30} GiB" if size >= 1 << 30 else f"{size >> 20} MiB"
+    return f"state ({human}) {'larger than' if size > 126 * 10**6 else 'fits in'} L2"
 
 
 def measured_peaks():
@@ -263,7 +272,8 @@ def run_reference(args, ws, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic seeded circuit (splitmix64 0xC2)",
-            "config": {"workload": WORKLOAD, "qubits": args.qubits, "depth": args.depth},
+            "config": {"workload": workload(args.qubits, args.depth, int(len(gates))),
+                       "qubits": args.qubits, "depth": args.depth},
             "cpu_baseline": {"value": val, "unit": "circuits/s", "cores": cores, "kind": kind,
                              "sample": sample},
             "e2e": {"value": val, "unit": "circuits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -422,8 +432,8 @@ def run_b200(args, ws, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic seeded circuit (splitmix64 0xC2)",
-            "config": {"workload": WORKLOAD, "qubits": n, "depth": args.depth, "path": "plain c128 tiled",
-                       "parallelism": f"replicas x{ws}", "l2": "state (16 GiB) larger than L2",
+            "config": {"workload": workload(n, args.depth, int(len(gates))), "qubits": n, "depth": args.depth,
+                       "path": "plain c128 tiled", "parallelism": f"replicas x{ws}", "l2": l2_note(n),
                        "tile_passes_per_circuit": passes, "gates": int(len(gates))},
             "hbm_gbs_per_pass": achieved,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
