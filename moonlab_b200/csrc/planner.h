@@ -63,7 +63,7 @@ struct Planner {
   // with dense_limits: a pass's last register segment of at most this many
   // ops goes back to the remaining ops (it would cost a whole dense segment;
   // the next pass usually takes it into one of its segments)
-  int defer_tail = 6;
+  int defer_tail = 12;
   std::vector<PlannedPass> passes;
   std::vector<DevSegment> segs;
   std::vector<DevOp> dops;
