@@ -311,6 +311,47 @@ int  mlb_server_wait(mlb_server_t *s, uint64_t ticket, int timeout_ms, uint64_t 
 int  mlb_server_get_stats(mlb_server_t *s, mlb_server_stats_t *out);
 void mlb_server_destroy(mlb_server_t *s);
 
+/* ---- persistent request loop for small circuits (a mailbox) ---------------
+ * One long-running launch serves small requests (<= 12 qubits complex128,
+ * <= 13 complex64, one dtype per mailbox) as they are posted: submit copies
+ * the request into a device-memory ring slot and publishes it; `ctas`
+ * thread blocks (one SM each; default 8, the rest of the GPU stays free for
+ * other work) claim published requests, run them with the state in shared
+ * memory and write the outcomes into mapped host memory, which
+ * mlb_mailbox_wait polls.  Shots follow moonlab_qgtl_execute exactly as in
+ * mlb_server_*: bit-identical outcomes for a non-zero rng_seed.  The loop's
+ * waits are bounded: after idle_ms (default 1000) without a request its
+ * blocks exit and the launch ends with MLB_ERR_TIMEOUT (counted in
+ * idle_exits); the next submit, or a waiter whose request is pending,
+ * relaunches it.  submit returns MLB_ERR_BUSY when all `slots` (default 64)
+ * hold unwaited tickets; a request with more than max_ops ops after fusion
+ * (default 2048) or max_shots shots (default 4096) is refused
+ * (MLB_ERR_INVALID_ARG).  wait: timeout_ms < 0 waits without limit, else
+ * MLB_ERR_TIMEOUT when it runs out (the ticket stays valid).  free stops the
+ * loop (it finishes the request in hand) and releases everything; tickets
+ * not yet waited are dropped. */
+typedef struct mlb_mailbox mlb_mailbox_t;
+typedef struct {
+    int32_t  dtype;      /* MLB_C128 or MLB_C64 */
+    int32_t  device;
+    int32_t  ctas;       /* 0: 8 */
+    uint32_t slots;      /* 0: 64 */
+    uint32_t max_ops;    /* 0: 2048 */
+    uint32_t max_shots;  /* 0: 4096 */
+    double   idle_ms;    /* 0: 1000 */
+} mlb_mailbox_config_t;
+typedef struct {
+    uint64_t submitted, completed;
+    uint64_t launches;    /* launches of the request loop */
+    uint64_t idle_exits;  /* launches that ended on the idle limit (MLB_ERR_TIMEOUT) */
+    uint64_t running;     /* 1 while a launch is live */
+} mlb_mailbox_stats_t;
+int mlb_mailbox_create(const mlb_mailbox_config_t *cfg, mlb_mailbox_t **out);
+int mlb_mailbox_submit(mlb_mailbox_t *mb, const mlb_request_t *req, uint64_t *ticket);
+int mlb_mailbox_wait(mlb_mailbox_t *mb, uint64_t ticket, int timeout_ms, uint64_t *outcomes, size_t capacity);
+int mlb_mailbox_get_stats(mlb_mailbox_t *mb, mlb_mailbox_stats_t *out);
+int mlb_mailbox_free(mlb_mailbox_t *mb);
+
 /* ---- control-plane front end ----------------------------------------------
  * The request execution of the reference's control server
  * (src/control/control_plane.c:598-770) on the device loop: one request

@@ -251,6 +251,27 @@ int launch_small_circuits(int dtype, const SmallItem* d_items, int num_items, co
 // of mlb_run_gates would plan).
 int prepare_ops(const mlb_gate_t* gates, size_t num_gates, uint32_t n, std::vector<mlb_op_t>& out);
 
+// ---- persistent small-circuit loop (kernels_mailbox.cu; mailbox.cpp) ----
+struct MailboxItem {  // one request, in ring slot seq % slots
+  uint32_t num_ops, n, shots, pad;
+};
+struct MailboxDev {
+  const MailboxItem* items;        // [slots]
+  const mlb_op_t* ops;             // [slots][max_ops]
+  const double* uniforms;          // [slots][max_shots]
+  unsigned long long* outcomes;    // mapped host memory, [slots][max_shots]
+  uint64_t* done;                  // mapped host memory, [slots]: seq + 1 once slot's request is done
+  uint64_t* head;                  // next sequence number to claim
+  const uint64_t* tail;            // requests published so far
+  const uint32_t* stop;            // non-zero: blocks exit
+  uint32_t* exited;                // blocks that have left this launch
+  int* end_status;                 // MLB_OK (stopped) or MLB_ERR_TIMEOUT (idle limit), by the last block
+  uint64_t idle_ns;
+  uint32_t slots, max_ops, max_shots, nmax;
+};
+size_t mailbox_smem_bytes(int dtype);
+int launch_mailbox(int dtype, const MailboxDev& mb, int ctas, cudaStream_t stream);
+
 // d_err: device word set non-zero if a tensor-core completion wait ran out.
 int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,
                       const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream, int test_skip_copy = 0);

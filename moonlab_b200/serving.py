@@ -6,7 +6,9 @@ requests that arrive while others run overlap with them on the device.
 `run_load` replays a Poisson request stream (circuits.config_c5) against a
 server in real time and reports throughput and latency percentiles.
 `ControlFrontEnd` puts the reference control server's request frames
-(HEALTH / CIRCUIT / SHOTS) onto the same loop.
+(HEALTH / CIRCUIT / SHOTS) onto the same loop.  `Mailbox` is the persistent
+request loop for small circuits (mlb_mailbox_*): one long-running launch
+serves posted requests without a launch per request.
 """
 from __future__ import annotations
 
@@ -42,7 +44,21 @@ class MlbServerStats(C.Structure):
                                           "plan_cache_hits")]
 
 
+class MlbMailboxConfig(C.Structure):
+    _fields_ = [("dtype", C.c_int32), ("device", C.c_int32), ("ctas", C.c_int32), ("slots", C.c_uint32),
+                ("max_ops", C.c_uint32), ("max_shots", C.c_uint32), ("idle_ms", C.c_double)]
+
+
+class MlbMailboxStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "launches", "idle_exits", "running")]
+
+
 _SIGS = {
+    "mlb_mailbox_create": (C.c_int, [C.POINTER(MlbMailboxConfig), C.POINTER(C.c_void_p)]),
+    "mlb_mailbox_submit": (C.c_int, [C.c_void_p, C.POINTER(MlbRequest), C.POINTER(C.c_uint64)]),
+    "mlb_mailbox_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(C.c_uint64), C.c_size_t]),
+    "mlb_mailbox_get_stats": (C.c_int, [C.c_void_p, C.POINTER(MlbMailboxStats)]),
+    "mlb_mailbox_free": (C.c_int, [C.c_void_p]),
     "mlb_server_create": (C.c_int, [C.c_int, C.c_size_t, C.c_int, C.POINTER(C.c_void_p)]),
     "mlb_server_submit": (C.c_int, [C.c_void_p, C.POINTER(MlbRequest), C.POINTER(C.c_uint64)]),
     "mlb_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(C.c_uint64), C.c_size_t,
@@ -104,6 +120,62 @@ class Server:
         if self._h:
             self._lib.mlb_server_destroy(self._h)
             self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Mailbox:
+    """The persistent request loop for small circuits (<= 12 qubits
+    complex128, <= 13 complex64; one dtype per mailbox): `ctas` thread blocks
+    of one long-running launch serve requests as they are posted.  The loop
+    ends itself after idle_ms without work (a bounded wait; counted in
+    stats()["idle_exits"]) and is relaunched by the next submit.  submit
+    raises MlbError(MLB_ERR_BUSY) when every slot holds an unwaited ticket."""
+
+    def __init__(self, dtype: str = "c128", device: int = 0, ctas: int = 0, slots: int = 0,
+                 max_ops: int = 0, max_shots: int = 0, idle_ms: float = 0.0):
+        self._lib = _bind()
+        cfg = MlbMailboxConfig(DTYPES[dtype], device, ctas, slots, max_ops, max_shots, idle_ms)
+        h = C.c_void_p()
+        check(self._lib.mlb_mailbox_create(C.byref(cfg), C.byref(h)), "mlb_mailbox_create")
+        self._h, self._dtype = h, DTYPES[dtype]
+        self._shots = {}
+
+    def submit(self, num_qubits: int, gates: np.ndarray, shots: int, seed: int) -> int:
+        g = np.ascontiguousarray(gates, dtype=GATE_DTYPE)
+        req = MlbRequest(num_qubits, self._dtype, g.ctypes.data, len(g), shots, 0, seed)
+        t = C.c_uint64()
+        check(self._lib.mlb_mailbox_submit(self._h, C.byref(req), C.byref(t)), "mlb_mailbox_submit")
+        self._shots[t.value] = shots
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> np.ndarray:
+        """Outcomes uint64[shots]; TimeoutError if not done in time (the
+        ticket stays valid)."""
+        shots = self._shots[ticket]
+        out = np.empty(max(shots, 1), dtype=np.uint64)
+        rc = self._lib.mlb_mailbox_wait(self._h, ticket, timeout_ms, out.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                        len(out))
+        if rc == -7:
+            raise TimeoutError(f"request {ticket} not done after {timeout_ms} ms")
+        check(rc, "mlb_mailbox_wait")
+        del self._shots[ticket]
+        return out[:shots]
+
+    def stats(self) -> dict:
+        s = MlbMailboxStats()
+        check(self._lib.mlb_mailbox_get_stats(self._h, C.byref(s)), "mlb_mailbox_get_stats")
+        return {k: int(getattr(s, k)) for k, _ in MlbMailboxStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            rc = self._lib.mlb_mailbox_free(self._h)
+            self._h = None
+            check(rc, "mlb_mailbox_free")
 
     def __enter__(self):
         return self
