@@ -54,11 +54,8 @@ typedef int moonlab_cuda_status_t;               /* cuda_statevec.h:39-46   */
 
 /* ---- GPU-backed quantum_state_t (src/quantum/state.h:437-464;
  *      reference definitions src/quantum/state_gpu.cu:31-98).
- *      create_gpu accepts 1..33 qubits (reference: 1..31).  The host mirror
- *      (amplitudes) is NULL until the first sync_to_host allocates and fills
- *      it: the mirror is stale until a sync in the reference too, and a
- *      state that is never read back takes no host memory (128 GiB at 33
- *      qubits).  sync_from_host with no mirror yet is a no-op success. ---- */
+ *      create_gpu accepts 1..33 qubits (reference: 1..31); the host mirror is
+ *      calloc'ed as in the reference, so untouched pages cost no memory. ---- */
 qs_error_t quantum_state_create_gpu(size_t num_qubits, quantum_state_t **out_state);
 qs_error_t quantum_state_sync_to_host(quantum_state_t *state);
 qs_error_t quantum_state_sync_from_host(quantum_state_t *state);

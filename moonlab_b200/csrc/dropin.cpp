@@ -23,14 +23,9 @@ int route(int rc) { return rc == MLB_OK ? 0 : -1; }
 extern "C" {
 
 // ---- GPU-backed quantum_state_t ----------------------------------------------
-// state_gpu.cu:31-72: opaque engine state in gpu_state, gpu_backend = 1.
-// The host mirror is allocated by the first quantum_state_sync_to_host
-// (amplitudes is NULL until then): the mirror is stale until a sync anyway
-// (state.h:117-130), and a state that is never read back -- a 33-qubit one
-// would need 128 GiB -- then takes no host memory, and the core's
-// quantum_state_free (which zeroes a mirror before freeing it) has nothing
-// to zero.  Errors: no device -> NOT_SUPPORTED, allocation failure ->
-// OUT_OF_MEMORY.
+// state_gpu.cu:31-72: calloc'ed host mirror holding |0...0>, opaque engine
+// state in gpu_state, gpu_backend = 1.  Errors: no device -> NOT_SUPPORTED,
+// allocation failure -> OUT_OF_MEMORY.
 qs_error_t quantum_state_create_gpu(size_t num_qubits, quantum_state_t** out_state) {
   if (!out_state) return QS_ERROR_INVALID_PARAM;
   *out_state = nullptr;
@@ -39,13 +34,19 @@ qs_error_t quantum_state_create_gpu(size_t num_qubits, quantum_state_t** out_sta
   if (!s) return QS_ERROR_OUT_OF_MEMORY;
   s->num_qubits = num_qubits;
   s->state_dim = (size_t)1 << num_qubits;
-  s->amplitudes = nullptr;  // allocated on the first sync_to_host
+  s->amplitudes = calloc(s->state_dim, 2 * sizeof(double));
+  if (!s->amplitudes) {
+    free(s);
+    return QS_ERROR_OUT_OF_MEMORY;
+  }
+  static_cast<double*>(s->amplitudes)[0] = 1.0;
   s->owns_memory = 1;
   int dev = 0;
   cudaGetDevice(&dev);
   mlb_state* e = nullptr;
   const int rc = mlb_state_create((uint32_t)num_qubits, MLB_C128, dev, &e);
   if (rc != MLB_OK) {
+    free(s->amplitudes);
     free(s);
     return (rc == MLB_ERR_NO_DEVICE || rc == MLB_ERR_DRIVER) ? QS_ERROR_NOT_SUPPORTED : QS_ERROR_OUT_OF_MEMORY;
   }
@@ -55,24 +56,19 @@ qs_error_t quantum_state_create_gpu(size_t num_qubits, quantum_state_t** out_sta
   return QS_SUCCESS;
 }
 
-// state_gpu.cu:74-86; allocates the host mirror on first use
+// state_gpu.cu:74-86
 qs_error_t quantum_state_sync_to_host(quantum_state_t* state) {
   if (!state) return QS_ERROR_INVALID_PARAM;
   mlb_state* e = eng(state);
   if (!e) return QS_SUCCESS;
-  if (!state->amplitudes) {
-    state->amplitudes = malloc(state->state_dim * 2 * sizeof(double));  // fully written by the copy
-    if (!state->amplitudes) return QS_ERROR_OUT_OF_MEMORY;
-  }
   return mlb_state_copy_to_host(e, state->amplitudes) == MLB_OK ? QS_SUCCESS : QS_ERROR_DRIVER;
 }
 
-// state_gpu.cu:88-98; with no host mirror yet the device state is the only
-// copy, so there is nothing to push
+// state_gpu.cu:88-98
 qs_error_t quantum_state_sync_from_host(quantum_state_t* state) {
   if (!state) return QS_ERROR_INVALID_PARAM;
   mlb_state* e = eng(state);
-  if (!e || !state->amplitudes) return QS_SUCCESS;
+  if (!e) return QS_SUCCESS;
   return mlb_state_copy_from_host(e, state->amplitudes) == MLB_OK ? QS_SUCCESS : QS_ERROR_DRIVER;
 }
 
