@@ -55,7 +55,10 @@ typedef int moonlab_cuda_status_t;               /* cuda_statevec.h:39-46   */
 /* ---- GPU-backed quantum_state_t (src/quantum/state.h:437-464;
  *      reference definitions src/quantum/state_gpu.cu:31-98).
  *      create_gpu accepts 1..33 qubits (reference: 1..31); the host mirror is
- *      calloc'ed as in the reference, so untouched pages cost no memory. ---- */
+ *      calloc'ed as in the reference (the core's gate_* functions refuse a
+ *      NULL amplitudes pointer before routing, gates.c:124), and pages of a
+ *      block that large are mapped on demand, so the mirror takes host
+ *      memory only where sync_to_host has written it. ---- */
 qs_error_t quantum_state_create_gpu(size_t num_qubits, quantum_state_t **out_state);
 qs_error_t quantum_state_sync_to_host(quantum_state_t *state);
 qs_error_t quantum_state_sync_from_host(quantum_state_t *state);

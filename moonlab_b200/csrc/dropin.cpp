@@ -24,8 +24,13 @@ extern "C" {
 
 // ---- GPU-backed quantum_state_t ----------------------------------------------
 // state_gpu.cu:31-72: calloc'ed host mirror holding |0...0>, opaque engine
-// state in gpu_state, gpu_backend = 1.  Errors: no device -> NOT_SUPPORTED,
-// allocation failure -> OUT_OF_MEMORY.
+// state in gpu_state, gpu_backend = 1.  The mirror cannot be left out until
+// the first sync: the core's gate functions refuse a state whose amplitudes
+// pointer is NULL before they route to the device (gates.c:124, :157, ...).
+// calloc maps a block this large on demand, so the mirror's pages take host
+// memory only once sync_to_host writes them (the page holding amplitude 0
+// aside).  Errors: no device -> NOT_SUPPORTED, allocation failure ->
+// OUT_OF_MEMORY.
 qs_error_t quantum_state_create_gpu(size_t num_qubits, quantum_state_t** out_state) {
   if (!out_state) return QS_ERROR_INVALID_PARAM;
   *out_state = nullptr;
