@@ -76,11 +76,10 @@ def fp64_tensor_peak(local: int):
 
 def profiled_traffic(n: int):
     """DRAM bytes of one k_tile<double> pass at n qubits: the ncu figure of
-    bytes per amplitude (profiles/k_tile_c128_traffic.json, dram read + write
-    of a 26-qubit pass, from the capture summarised in
-    profiles/k_tile_c128_26q.md) times 2^n.  A pass moves every amplitude once
-    each way, so its traffic grows in proportion to 2^n.  None if the file is
-    gone."""
+    bytes per amplitude (profiles/k_tile_c128_traffic.json: dram read + write
+    of a 26-qubit pass, the capture command inside the file) times 2^n.  A
+    pass moves every amplitude once each way, so its traffic grows in
+    proportion to 2^n.  None if the file is gone."""
     p = ROOT / "profiles" / "k_tile_c128_traffic.json"
     if not p.exists():
         return None
