@@ -505,6 +505,7 @@ def serving_leg(args, local, with_cpu: bool):
             _, info = srv.wait(srv.submit(r.n, circ[i], r.shots, r.seed, "c64" if r.dtype else "c128"))
             gpu_alone.append(info["done_s"] - info["submit_s"])
     meets = [x["rate_per_s"] for x in sweep if x["p99_ms"] <= p99_target_ms]
+    small_leg = small_requests_leg(local)
     cpu = None
     if with_cpu:
         try:  # the reference's moonlab_qgtl_execute on the same small requests (all host threads)
@@ -537,7 +538,34 @@ def serving_leg(args, local, with_cpu: bool):
         "max_rate_meeting_p99_per_s": max(meets) if meets else None,
         "small_batches": paced["stats"]["small_batches"], "plan_cache_hits": paced["stats"]["plan_cache_hits"],
         "cpu_reference": cpu,
+        "small_requests": small_leg,
     }
+
+
+def small_requests_leg(local, num: int = 1000, rate: float = 200.0):
+    """Small requests alone (8..12 qubits complex128, depth U{10..100}
+    brickwork, shots U{1..4096}, Poisson at `rate`/s): the batch launches of
+    mlb_server_* against the persistent loop (mlb_mailbox_*), p50/p99
+    latency from submit to result on the host clock."""
+    from moonlab_b200.circuits import Request
+    from moonlab_b200.serving import Mailbox, Server, request_circuit, run_load, run_mailbox_load
+    rng = np.random.default_rng(0x5A11)
+    gaps = rng.exponential(1.0 / rate, num)
+    reqs = [Request(i, float(t), int(rng.integers(8, 13)), int(rng.integers(10, 101)), int(rng.integers(1, 4097)),
+                    0, int(rng.integers(1, 2**62))) for i, t in enumerate(np.cumsum(gaps))]
+    circ = [request_circuit(r) for r in reqs]
+    with Server(device=local, workers=8) as srv:
+        run_load(srv, reqs[:50], time_scale=0.0, circuits=circ[:50])  # warm-up
+        batch = run_load(srv, reqs, time_scale=1.0, circuits=circ)
+    with Mailbox("c128", device=local, ctas=8) as mb:
+        run_mailbox_load(mb, reqs[:50], time_scale=0.0, circuits=circ[:50])
+        loop = run_mailbox_load(mb, reqs, time_scale=1.0, circuits=circ)
+    pick = lambda d: {"circuits_per_s": d["circuits_per_s"], "p50_ms": d["p50_s"] * 1e3, "p99_ms": d["p99_s"] * 1e3,
+                      "mean_ms": d["mean_s"] * 1e3}
+    return {"workload": f"{num} requests of 8..12 qubits (c128), depth U{{10..100}} brickwork, shots U{{1..4096}}, "
+                        f"Poisson at {rate:g}/s",
+            "batch_launches": pick(batch), "persistent_loop": dict(pick(loop), ctas=8,
+                                                                    launches=loop["stats"]["launches"])}
 
 
 def gate_sweep_leg(local, peak):

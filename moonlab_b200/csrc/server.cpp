@@ -64,7 +64,8 @@ struct Request {
   std::vector<mlb_gate_t> gates;
   uint32_t shots = 0;
   uint64_t seed = 0;
-  int status = 1;  // 1 pending, 2 running, else final mlb_status_t
+  int status = 1;  // 1 pending, 2 running, else final mlb_status_t (written under mu)
+  int result = 0;  // a small batch's outcome for this request, published as status under mu
   std::vector<uint64_t> outcomes;
   double t_submit = 0, t_admit = 0, t_done = 0;
   size_t bytes = 0;
@@ -227,7 +228,8 @@ struct mlb_server {
     return MLB_OK;
   }
 
-  // Runs a batch of small requests in one launch; sets each one's status.
+  // Runs a batch of small requests in one launch; sets each one's result
+  // (the caller publishes it as the status, with the completion time).
   void run_small(std::vector<Request*>& batch, SmallBufs& B) {
     const int dtype = batch[0]->dtype;
     std::vector<mlb::SmallItem> items;
@@ -239,7 +241,7 @@ struct mlb_server {
       std::vector<mlb_op_t> o;
       const int rc = mlb::prepare_ops(r->gates.data(), r->gates.size(), r->n, o);
       if (rc) {
-        r->status = rc;
+        r->result = rc;
         continue;
       }
       mlb::SmallItem it{};
@@ -282,7 +284,7 @@ struct mlb_server {
     for (size_t i = 0; i < live.size(); i++) {
       Request* r = live[i];
       if (!rc) r->outcomes.assign(out.begin() + items[i].out_off, out.begin() + items[i].out_off + r->shots);
-      r->status = rc;
+      r->result = rc;
     }
   }
 
@@ -325,8 +327,11 @@ struct mlb_server {
         run_small(batch, sbufs);
         lk.lock();
         running -= (int)batch.size();
+        // outcome and completion time become visible together, under mu: a
+        // waiter may take (and delete) a request as soon as its status is final
         const double td = now();
         for (Request* q : batch) {
+          q->status = q->result;
           q->t_done = td;
           if (q->status) st.failed++;
           st.completed++;

@@ -184,6 +184,53 @@ class Mailbox:
         self.close()
 
 
+def run_mailbox_load(mb: "Mailbox", requests, time_scale: float = 1.0, circuits=None):
+    """run_load for the persistent loop: submit at the arrival times from one
+    thread, collect in order in another.  A request's latency is submit to
+    the return of its wait on the host clock.  A submit refused because every
+    slot holds a ticket is retried after 50 us."""
+    circuits = circuits if circuits is not None else [request_circuit(r) for r in requests]
+    tickets = [None] * len(requests)
+    t_sub = [0.0] * len(requests)
+    ready = [threading.Event() for _ in requests]
+    errors = []
+
+    def producer():
+        t0 = time.perf_counter()
+        for i, r in enumerate(requests):
+            delay = r.arrival * time_scale - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            while True:
+                try:
+                    t_sub[i] = time.perf_counter()
+                    tickets[i] = mb.submit(r.n, circuits[i], r.shots, r.seed)
+                    break
+                except _lib.MlbError as e:
+                    if e.status != -8:  # MLB_ERR_BUSY: retry
+                        errors.append((i, e))
+                        break
+                    time.sleep(50e-6)
+            ready[i].set()
+
+    t_done = [0.0] * len(requests)
+    th = threading.Thread(target=producer)
+    th.start()
+    for i in range(len(requests)):
+        ready[i].wait()
+        if tickets[i] is not None:
+            mb.wait(tickets[i])
+            t_done[i] = time.perf_counter()
+    th.join()
+    if errors:
+        raise RuntimeError(f"{len(errors)} submissions failed; first: {errors[0]}")
+    lat = np.array([d - s for s, d in zip(t_sub, t_done)])
+    span = max(t_done) - min(t_sub)
+    return {"circuits_per_s": len(requests) / span, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "span_s": span,
+            "stats": mb.stats()}
+
+
 class ControlFrontEnd:
     """The control server's request execution on the device loop
     (mlb_control_*): `handle(frame)` takes one request frame of the

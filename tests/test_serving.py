@@ -122,8 +122,12 @@ def test_small_requests_share_launches(gpu):
             alone.append(s.wait(s.submit(n, g, shots, seed, dt))[0])
     with Server(workers=2) as s:
         tickets = [s.submit(*r) for r in reqs]
-        mixed = [s.wait(t)[0] for t in tickets]
+        done = [s.wait(t) for t in tickets]
         st = s.stats()
+    mixed = [d[0] for d in done]
+    # a request's times are final when its result is: submit <= admit <= done
+    for _, info in done:
+        assert 0.0 <= info["submit_s"] <= info["admit_s"] <= info["done_s"]
     assert st["small_requests"] == len(reqs)
     assert st["small_batches"] < len(reqs)
     for a, b in zip(alone, mixed):
