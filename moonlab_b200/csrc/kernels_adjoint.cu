@@ -21,6 +21,9 @@
 //                 X-part lies inside the tile; the last pass also emits the
 //                 per-tile partial of Re<psi|lambda> (the energy).
 //   k_adj_reduce: fixed-order sums of the per-tile partials (deterministic).
+// Tiles come into shared memory by asynchronous copies, all in flight at
+// once.  (Issuing the next tile's copies from the store loop, as the state
+// engine's tile passes do, measured no faster here.)
 #include <cstdio>
 
 #include "kernels_common.cuh"
@@ -45,13 +48,29 @@ __device__ __forceinline__ uint64_t tile_base_of(const AdjPass& P, uint64_t tile
   return (b << P.n) | pdep64(t, P.tile_free_mask);
 }
 
+// HBM -> shared by asynchronous copies: every load of the tile is in flight
+// at once (a load-then-store loop would wait out each load's latency in
+// turn).  The caller completes them with tile_loads_wait() and a barrier.
 template <typename Real>
 __device__ __forceinline__ void load_tile(typename Cplx<Real>::T* __restrict__ sm,
                                           const typename Cplx<Real>::T* __restrict__ g,
                                           uint64_t tile_base, const uint64_t* rowoff, int L, uint32_t amps) {
+  using A = typename Cplx<Real>::T;
   constexpr int NT = AdjCfg<Real>::NT;
   const uint32_t lm = (1u << L) - 1u;
-  for (uint32_t e = threadIdx.x; e < amps; e += NT) sm[aswz<Real>(e)] = __ldcs(&g[tile_base | rowoff[e >> L] | (e & lm)]);
+  const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
+#pragma unroll 1
+  for (uint32_t e = threadIdx.x; e < amps; e += NT) {
+    const A* src = &g[tile_base | rowoff[e >> L] | (e & lm)];
+    const uint32_t dst = base + aswz<Real>(e) * (uint32_t)sizeof(A);
+    if constexpr (sizeof(A) == 16)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    else
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+  }
+}
+__device__ __forceinline__ void tile_loads_wait() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 template <typename Real>
 __device__ __forceinline__ void store_tile(const typename Cplx<Real>::T* __restrict__ sm,
@@ -159,6 +178,7 @@ __global__ void __launch_bounds__(AdjCfg<Real>::NT, 2)
     for (int i = threadIdx.x; i < (NT / 32) * kMaxAdjSlots; i += NT) (&red[0][0])[i] = 0.0;
     load_tile<Real>(sv, psi, tb, rowoff, P.L, amps);
     if (DUAL) load_tile<Real>(sw, lam, tb, rowoff, P.L, amps);
+    tile_loads_wait();
     __syncthreads();
 
     for (int s = 0; s < P.num_segments; s++) {
@@ -288,6 +308,7 @@ __global__ void __launch_bounds__(AdjCfg<Real>::NT, 1)
   for (uint64_t tile = blockIdx.x; tile < P.num_tiles; tile += gridDim.x) {
     const uint64_t tb = tile_base_of(P, tile);
     load_tile<Real>(sv, psi, tb, rowoff, P.L, amps);
+    tile_loads_wait();
     __syncthreads();
     double e_acc = 0.0;
     for (uint32_t e = threadIdx.x; e < amps; e += NT) {
