@@ -282,11 +282,32 @@ inline int emit(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P,
         if (std::find(pos.begin(), pos.end(), t) == pos.end()) pos.push_back(t);
       std::sort(pos.begin(), pos.end());
       FusedBlockDev db{};
-      int qi = 0;
+      std::vector<int> rows;  // the tile bits outside the block: a thread's row index m
       for (int t = 0; t < kTileBits; t++) {
         const auto it = std::find(pos.begin(), pos.end(), t);
         if (it != pos.end()) db.pos[it - pos.begin()] = (uint8_t)t;
-        else db.q[qi++] = (uint8_t)t;
+        else rows.push_back(t);
+      }
+      // Row bits 0..3 are the lanes of one shared-memory phase (16 lanes of
+      // 8-byte accesses; 8 lanes of 16-byte pair accesses when tile bit 0 is
+      // the block's first column bit).  Under the kernel's tile swizzle, tile
+      // bit t moves a float2's bank-pair index (bits 0..3) along bit
+      // class(t): t = 0 -> 0; t = 1, 5, 9 -> 1; 2, 6, 10 -> 2; 3, 7, 11 -> 3;
+      // 4, 8, 12 -> none.  Putting one row bit of each class first makes the
+      // phase's lanes hit distinct banks.
+      {
+        auto cls = [](int t) { return t == 0 ? 0 : (t % 4 == 0) ? -1 : (t - 1) % 4 + 1; };
+        const bool pairs = pos[0] == 0;
+        std::vector<int> order;
+        for (int want = pairs ? 1 : 0; want <= 3; want++)
+          for (int t : rows)
+            if (cls(t) == want && std::find(order.begin(), order.end(), t) == order.end()) {
+              order.push_back(t);
+              break;
+            }
+        for (int t : rows)
+          if (std::find(order.begin(), order.end(), t) == order.end()) order.push_back(t);
+        for (int i = 0; i < (int)order.size(); i++) db.q[i] = (uint8_t)order[i];
       }
       // local bit of each global qubit: the index of its tile position in pos
       int lb[64];
