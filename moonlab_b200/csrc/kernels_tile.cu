@@ -395,6 +395,18 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, DENSE ? 3 : TileCfg<Real>::
   // the stores instead of following them.
   const bool full = tile_amps == (1u << TB);
   const uint32_t sm_base = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
+  // Row offset of element e = threadIdx.x + j NT of a full tile: NT is a
+  // multiple of the row length 2^L (or the tile has no high bits and every
+  // row offset is 0), so e >> L = (threadIdx.x >> L) | (j NT >> L) on
+  // disjoint bits and the offset is this thread's part OR a part that is
+  // the same for every thread (a broadcast read instead of a per-lane one).
+  // Used for complex128 (measured 1.6 % faster there, 1.4 % slower for
+  // complex64's 5-bit rows).
+  const uint64_t my_row = rowoff[threadIdx.x >> L];
+  auto row_of = [&](uint32_t e, int j) -> uint64_t {
+    if constexpr (sizeof(Real) == 8) return my_row | rowoff[(uint32_t)(j * NT) >> L];
+    else return rowoff[e >> L];
+  };
   bool prefetched = false;
   uint32_t dq = 0;  // dense-only passes: segment applications so far (staging slot parity)
   for (uint64_t tile = blockIdx.x; tile < pass.num_tiles; tile += gridDim.x) {
@@ -419,7 +431,7 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, DENSE ? 3 : TileCfg<Real>::
 #pragma unroll
       for (int j = 0; j < PER; j++) {
         const uint32_t e = threadIdx.x + j * NT;
-        tmp[j] = __ldcs(&amp[tile_base | rowoff[e >> L] | (e & lmask_low)]);
+        tmp[j] = __ldcs(&amp[tile_base | row_of(e, j) | (e & lmask_low)]);
       }
 #pragma unroll
       for (int j = 0; j < PER; j++) sm[swz<Real>(threadIdx.x + j * NT)] = tmp[j];
@@ -534,7 +546,7 @@ __global__ void __launch_bounds__(TileCfg<Real>::NT, DENSE ? 3 : TileCfg<Real>::
       for (int j = 0; j < PER; j++) {
         const uint32_t e = threadIdx.x + j * NT;
         const uint32_t slot = swz<Real>(e);
-        const uint64_t off = rowoff[e >> L] | (e & lmask_low);
+        const uint64_t off = row_of(e, j) | (e & lmask_low);
         const A v = sm[slot];
         __stcs(&amp[tile_base | off], v);  // consumes v: the slot has been read
         if (prefetched) {
