@@ -649,6 +649,8 @@ def vqe_leg(local, with_cpu: bool):
                        + 4 * ck)
         achieved = per_vec * len(prob.params) / t / 1e9
         res[dt] = {"vectors_per_s": len(prob.params) / t, "batch_ms": t * 1e3,
+                   "path": (f"{dt} adjoint tile passes on the CUDA cores (the fused tensor-core path is not used "
+                            "for the adjoint)"),
                    "timing": "median of 3 calls after a full-batch warm-up (host parameters in, host "
                              "energies and gradients out)",
                    "passes": ps, "checkpoints": ev,
