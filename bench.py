@@ -625,8 +625,11 @@ def vqe_leg(local, with_cpu: bool):
     res = {"workload": "HEA N=20 L=8 (320 parameters), 80 2-local Pauli terms, batch 256"}
     grads = {}
     peak, peak_kind = measured_peaks()
-    for dt in ("c128", "c64"):
-        p = HEAProblem(20, 8, prob.coeffs, xmasks=prob.xmasks, zmasks=prob.zmasks, dtype=dt, device=local)
+    for dt in ("c128", "c64", "c64_cuda_core_forward"):
+        p = HEAProblem(20, 8, prob.coeffs, xmasks=prob.xmasks, zmasks=prob.zmasks,
+                       dtype="c128" if dt == "c128" else "c64", device=local)
+        if dt == "c64_cuda_core_forward":
+            p.set_fused_forward("off")
         p.evaluate(prob.params)  # warm-up at the full batch: workspaces are sized by the first call
         times = []
         for _ in range(3):
@@ -645,12 +648,14 @@ def vqe_leg(local, with_cpu: bool):
         ck = 0
         if ev["checkpoints"]:
             ck = -(-8 // ev["segment_layers"]) - 1  # segments - 1
-        per_vec = S * (2 * ps["forward_passes"] + 2 + 3 * (ps["lambda_passes"] - 1) + 4 * ps["backward_passes"]
-                       + 4 * ck)
+        fwd = ev["fused_forward_passes"] if ev["fused_forward"] else ps["forward_passes"]
+        per_vec = S * (2 * fwd + 2 + 3 * (ps["lambda_passes"] - 1) + 4 * ps["backward_passes"] + 4 * ck)
         achieved = per_vec * len(prob.params) / t / 1e9
-        res[dt] = {"vectors_per_s": len(prob.params) / t, "batch_ms": t * 1e3,
-                   "path": (f"{dt} adjoint tile passes on the CUDA cores (the fused tensor-core path is not used "
-                            "for the adjoint)"),
+        path = ("complex128 adjoint tile passes on the CUDA cores" if dt == "c128" else
+                "complex64: forward sweep on the tensor cores (fused <= 5-qubit blocks, per-vector operand "
+                "images built on the device), lambda and backward passes on the CUDA cores"
+                if ev["fused_forward"] else "complex64 adjoint tile passes on the CUDA cores")
+        res[dt] = {"vectors_per_s": len(prob.params) / t, "batch_ms": t * 1e3, "path": path,
                    "timing": "median of 3 calls after a full-batch warm-up (host parameters in, host "
                              "energies and gradients out)",
                    "passes": ps, "checkpoints": ev,
@@ -661,6 +666,8 @@ def vqe_leg(local, with_cpu: bool):
         p.close()
     res["c64_max_rel_grad_err"] = float(np.abs(grads["c64"] - grads["c128"]).max() /
                                         max(1e-300, np.abs(grads["c128"]).max()))
+    res["c64_cuda_core_forward_max_rel_grad_err"] = float(
+        np.abs(grads["c64_cuda_core_forward"] - grads["c128"]).max() / max(1e-300, np.abs(grads["c128"]).max()))
     if with_cpu:  # the reference's moonlab_vqe_gradient at N = 12 (minutes per vector at N = 20)
         try:
             from oracle import bindings as B

@@ -534,6 +534,19 @@ int  mlb_hea_set_checkpointing(mlb_hea_t *h, int mode);
  * checkpoints, and how many sub-batches it ran. */
 int  mlb_hea_last_eval_stats(const mlb_hea_t *h, uint32_t *segment_layers, int *checkpoints_used,
                              size_t *sub_batches);
+/* complex64 problems with N >= 13: the forward sweep runs on the tensor
+ * cores -- each checkpoint segment's gates grouped into <= 5-qubit blocks
+ * and applied by the fused complex64 kernel, with every vector's operand
+ * images built on the device from its angles.  The FP32 accumulation shrinks
+ * |psi| by ~4e-7 per block, so energies and gradients are divided by the
+ * forward state's squared norm (both carry it).  mode 0 (default): on for
+ * complex64 when the plan exists; 1: on (MLB_ERR_NOT_SUPPORTED without a
+ * plan); -1: off (the CUDA-core forward passes).  The backward sweep always
+ * runs on the CUDA cores.  *fused: whether the last evaluation used it;
+ * *passes, *blocks: the fused forward plan's passes and blocks (0 without a
+ * plan); any output may be NULL. */
+int  mlb_hea_set_fused_forward(mlb_hea_t *h, int mode);
+int  mlb_hea_last_forward_fused(const mlb_hea_t *h, int *fused, uint32_t *passes, uint32_t *blocks);
 /* Quantum geometry at one parameter vector (complex128 problems): the
  * Fubini-Study metric g = Re Q and the Berry curvature F = -2 Im Q of
  * Q_ij = <d_i psi|d_j psi> - <d_i psi|psi><psi|d_j psi>, each P x P

@@ -158,6 +158,9 @@ _SIGS = {
                                      C.POINTER(C.c_uint32)]),
     "mlb_hea_last_error": (C.c_char_p, []),
     "mlb_hea_set_checkpointing": (C.c_int, [C.c_void_p, C.c_int]),
+    "mlb_hea_set_fused_forward": (C.c_int, [C.c_void_p, C.c_int]),
+    "mlb_hea_last_forward_fused": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_uint32)]),
     "mlb_hea_last_eval_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_int),
                                           C.POINTER(C.c_size_t)]),
     "moonlab_vqe_gradient": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_size_t]),

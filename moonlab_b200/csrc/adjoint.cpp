@@ -29,6 +29,7 @@
 #include <string>
 #include <vector>
 
+#include "fused.h"
 #include "mlb_internal.h"
 #include "planner.h"
 
@@ -106,6 +107,24 @@ struct mlb_hea {
   unsigned char* d_gram = nullptr;  // geometry: Gram matrix, then the Gram kernel's scratch
   size_t gram_cap = 0;
   size_t budget = 0;         // bytes for psi + lambda; 0 = 80% of free memory
+  // complex64 forward sweep on the tensor cores (N >= 13): per segment, fused
+  // passes of <= 5-qubit blocks whose operand images are built on the device
+  // per vector from the cos/sin table (k_fused_images)
+  int fused_mode = 0;        // 0 auto (complex64, N >= 13), 1 on, -1 off
+  bool fused_ok = false;     // the fused plans exist
+  int last_fused = 0;
+  std::vector<std::vector<FusedPassDev>> fseg;  // per forward segment
+  std::vector<FusedBlockDev> fblocks;           // image = the block's index among all segments' blocks
+  std::vector<FusedGenBlock> gblocks;
+  std::vector<FusedGenOp> gops;
+  FusedBlockDev* d_fblocks = nullptr;
+  FusedGenBlock* d_gblocks = nullptr;
+  FusedGenOp* d_gops = nullptr;
+  uint8_t* d_images = nullptr;
+  size_t images_cap = 0;     // bytes
+  int* d_ferr = nullptr;
+  double* d_norm = nullptr;
+  size_t norm_cap = 0;
 };
 
 namespace {
@@ -325,6 +344,60 @@ void plan_terms(mlb_hea* h) {
   }
 }
 
+// Fused plans of the forward sweep (complex64, N >= 13): each segment's gates
+// grouped into <= 5-qubit blocks and tile passes by the fused planner (on
+// stand-in ops: only their qubits matter), each block's gates recorded in
+// its local qubits for the device image builder.  False when a segment does
+// not plan (the CUDA-core forward passes then run).
+bool plan_fused_forward(mlb_hea* h, const std::vector<size_t>& cut) {
+  const uint32_t n = h->n;
+  if (n < (uint32_t)fused::kTileBits) return false;
+  for (size_t k = 0; k + 1 < cut.size(); k++) {
+    const std::vector<TapeOp> sub(h->tape.begin() + cut[k], h->tape.begin() + cut[k + 1]);
+    std::vector<mlb_op_t> ops;
+    ops.reserve(sub.size());
+    for (const TapeOp& t : sub) ops.push_back(proxy(t));
+    fused::Plan P;
+    if (fused::plan(ops, n, P) != MLB_OK) return false;
+    std::vector<FusedPassDev> passes;
+    size_t j = 0;  // P.dev_blocks are in pass order
+    for (size_t pi = 0; pi < P.passes.size(); pi++) {
+      FusedPassDev dp = P.dev_passes[pi];
+      dp.block_begin = (uint32_t)h->fblocks.size();
+      int tpos[64];
+      for (int& x : tpos) x = -1;
+      for (int q = 0; q < dp.num_low; q++) tpos[q] = q;
+      for (int i = 0; i < dp.num_high; i++) tpos[dp.hbits[i]] = dp.num_low + i;
+      for (int bi : P.passes[pi].blocks) {
+        FusedBlockDev db = P.dev_blocks[j++];
+        auto local = [&](int q) {
+          for (int c = 0; c < fused::kBlockQubits; c++)
+            if (tpos[q] >= 0 && db.pos[c] == tpos[q]) return c;
+          return -1;
+        };
+        FusedGenBlock gb{(uint32_t)h->gops.size(), 0};
+        for (int oi : P.blocks[bi].ops) {
+          const TapeOp& t = sub[oi];
+          FusedGenOp g{};
+          g.kind = (int8_t)t.kind;
+          g.lt = (int8_t)local(t.q);
+          g.lc = (int8_t)(t.ctrl >= 0 ? local(t.ctrl) : -1);
+          g.p = t.p;
+          if (g.lt < 0 || (t.ctrl >= 0 && g.lc < 0)) return false;
+          h->gops.push_back(g);
+          gb.num_ops++;
+        }
+        db.image = (uint32_t)h->fblocks.size();
+        h->fblocks.push_back(db);
+        h->gblocks.push_back(gb);
+      }
+      passes.push_back(dp);
+    }
+    h->fseg.push_back(std::move(passes));
+  }
+  return true;
+}
+
 int upload_programs(mlb_hea* h) {
   std::vector<AdjOp> all_ops;
   std::vector<int> all_slots;
@@ -348,7 +421,32 @@ int upload_programs(mlb_hea* h) {
   cudaMemcpy(h->d_slots, all_slots.data(), all_slots.size() * sizeof(int), cudaMemcpyHostToDevice);
   e = cudaMemcpy(h->d_terms, all_terms.data(), all_terms.size() * sizeof(AdjTerm), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return cfail(e, "adjoint program upload");
+  if (h->fused_ok) {
+    e = cudaMalloc((void**)&h->d_fblocks, h->fblocks.size() * sizeof(FusedBlockDev));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->d_gblocks, h->gblocks.size() * sizeof(FusedGenBlock));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->d_gops, std::max<size_t>(1, h->gops.size()) * sizeof(FusedGenOp));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->d_ferr, sizeof(int));
+    if (e != cudaSuccess) return cfail(e, "fused forward program upload");
+    cudaMemcpy(h->d_fblocks, h->fblocks.data(), h->fblocks.size() * sizeof(FusedBlockDev), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_gblocks, h->gblocks.data(), h->gblocks.size() * sizeof(FusedGenBlock), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(h->d_gops, h->gops.data(), h->gops.size() * sizeof(FusedGenOp), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cfail(e, "fused forward program upload");
+  }
   return MLB_OK;
+}
+
+// Bits of the tile enumeration of a batch of B states of n qubits.
+int batch_bits(uint32_t n, size_t B) {
+  int b = 0;
+  while (((size_t)1 << b) < B) b++;
+  return (int)n + b;
+}
+
+// Whether this evaluation runs the forward sweep on the tensor cores
+// (complex64 states only: the fused kernel works on FP32 amplitudes).
+bool use_fused_forward(const mlb_hea* h, size_t B) {
+  if (!h->fused_ok || h->fused_mode < 0 || h->dtype != MLB_C64) return false;
+  return batch_bits(h->n, B) <= 13 + 24 && B <= 65535;  // the fused kernel's tile-index reach
 }
 
 int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, double* h_G, bool use_ckpt) {
@@ -393,20 +491,55 @@ int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, do
   if ((rc = launch_adj_init(h->dtype, h->psi, (int)h->n, B, 0, h->stream))) return hfail(rc, "init kernel");
   const size_t nseg = h->fwd_seg.size() - 1;
   const size_t state_bytes = B * dim * ab;
+  const bool fused = use_fused_forward(h, B);
+  h->last_fused = fused ? 1 : 0;
+  if (fused) {  // every vector's operand images, from the cos/sin table
+    const size_t K = h->fblocks.size();
+    if (h->images_cap < B * K * fused::kBImageBytes) {
+      if (h->d_images) cudaFree(h->d_images);
+      h->d_images = nullptr;
+      h->images_cap = 0;
+      cudaError_t e = cudaMalloc((void**)&h->d_images, B * K * fused::kBImageBytes);
+      if (e != cudaSuccess) return cfail(e, "operand image allocation");
+      h->images_cap = B * K * fused::kBImageBytes;
+    }
+    if ((rc = launch_fused_images(h->d_gblocks, (int)K, h->d_gops, h->d_cs, (int)h->P, (int)B, h->d_images,
+                                  h->stream)))
+      return hfail(rc, "operand image build");
+    cudaMemsetAsync(h->d_ferr, 0, sizeof(int), h->stream);
+  }
   for (size_t k = 0; k < nseg; k++) {
-    for (size_t i = h->fwd_seg[k]; i < h->fwd_seg[k + 1]; i++) {
-      const GatePass& gp = h->fwd[i];
-      AdjPass P = gp.P;
-      P.num_tiles = P.tiles_per_state * B;
-      if ((rc = launch_adj_gates(h->dtype, h->psi, nullptr, P, h->d_ops + gp.ops_off, h->d_cs, nullptr, false,
-                                 false, h->num_sms, h->stream)))
-        return hfail(rc, "forward pass");
+    if (fused) {
+      for (FusedPassDev dp : h->fseg[k]) {
+        dp.num_tiles = (uint64_t)B << (h->n - fused::kTileBits);
+        dp.vec_shift = h->n - fused::kTileBits;
+        dp.vec_images = (uint32_t)h->fblocks.size();
+        if ((rc = launch_fused_pass(h->psi, batch_bits(h->n, B), dp, h->d_fblocks, h->d_images, h->d_ferr,
+                                    h->num_sms, h->stream)))
+          return hfail(rc, "fused forward pass");
+      }
+    } else {
+      for (size_t i = h->fwd_seg[k]; i < h->fwd_seg[k + 1]; i++) {
+        const GatePass& gp = h->fwd[i];
+        AdjPass P = gp.P;
+        P.num_tiles = P.tiles_per_state * B;
+        if ((rc = launch_adj_gates(h->dtype, h->psi, nullptr, P, h->d_ops + gp.ops_off, h->d_cs, nullptr, false,
+                                   false, h->num_sms, h->stream)))
+          return hfail(rc, "forward pass");
+      }
     }
     if (use_ckpt && k + 1 < nseg) {
       cudaError_t e = cudaMemcpyAsync((char*)h->ckpt + k * state_bytes, h->psi, state_bytes,
                                       cudaMemcpyDeviceToDevice, h->stream);
       if (e != cudaSuccess) return cfail(e, "checkpoint save");
     }
+  }
+  // The tensor-core forward shrinks |psi| slightly (its FP32 accumulation
+  // rounds magnitudes down); energies and gradients both carry |psi|^2, so
+  // they are divided by the forward state's squared norm at the end.
+  if (fused) {
+    if ((rc = grow(h->d_norm, h->norm_cap, B))) return rc;
+    if ((rc = launch_batch_norm(h->psi, dim, B, h->d_norm, h->stream))) return hfail(rc, "forward norm");
   }
   // 3. lambda = H psi and the energies
   for (size_t k = 0; k < h->lam.size(); k++) {
@@ -442,10 +575,15 @@ int evaluate_chunk(mlb_hea* h, size_t B, const double* h_params, double* h_E, do
     }
     }
   }
+  if (fused && (rc = launch_divide_by_norm(h->d_out, B, (int)h->P, h->d_norm, h->stream)))
+    return hfail(rc, "norm correction");
   if (h_E) cudaMemcpyAsync(h_E, h->d_out, B * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
   if (h_G) cudaMemcpyAsync(h_G, h->d_out + B, B * h->P * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  int ferr = 0;
+  if (fused) cudaMemcpyAsync(&ferr, h->d_ferr, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return cfail(e, "adjoint evaluation");
+  if (ferr) return hfail(MLB_ERR_TIMEOUT, "fused forward pass: tensor-core completion wait ran out");
   return MLB_OK;
 }
 
@@ -612,6 +750,16 @@ int mlb_hea_create(uint32_t n, uint32_t layers, uint64_t hf, size_t num_terms, c
     h->bwd_seg.push_back(h->bwd.size());
   }
   plan_terms(h);
+  // the tensor-core forward sweep's plans (used by complex64 problems by default)
+  if (dtype == MLB_C64 && h->n == n && n >= (uint32_t)fused::kTileBits) {
+    h->fused_ok = plan_fused_forward(h, cut);
+    if (!h->fused_ok) {
+      h->fseg.clear();
+      h->fblocks.clear();
+      h->gblocks.clear();
+      h->gops.clear();
+    }
+  }
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete h;
     return hfail(MLB_ERR_DRIVER, "stream creation");
@@ -630,7 +778,9 @@ void mlb_hea_free(mlb_hea_t* h) {
   Guard g(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (void* p : {h->psi, h->lamb, h->ckpt, (void*)h->d_cs, (void*)h->d_part, (void*)h->d_epart,
-                  (void*)h->d_ops, (void*)h->d_terms, (void*)h->d_slots, (void*)h->d_out, (void*)h->d_gram})
+                  (void*)h->d_ops, (void*)h->d_terms, (void*)h->d_slots, (void*)h->d_out, (void*)h->d_gram,
+                  (void*)h->d_fblocks, (void*)h->d_gblocks, (void*)h->d_gops, (void*)h->d_images,
+                  (void*)h->d_ferr, (void*)h->d_norm})
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -685,7 +835,8 @@ int mlb_hea_evaluate(mlb_hea_t* h, size_t batch, const double* params, double* e
   // checkpoints when they fit with the whole batch (mode 1: always; -1: never)
   bool use_ckpt = extra > 0 && grads != nullptr && h->ckpt_mode >= 0 &&
                   (h->ckpt_mode == 1 || budget / ((2 + extra) * sb) >= batch);
-  const size_t per = (2 + (use_ckpt ? extra : 0)) * sb;
+  const size_t img = use_fused_forward(h, batch) ? h->fblocks.size() * fused::kBImageBytes : 0;  // per vector
+  const size_t per = (2 + (use_ckpt ? extra : 0)) * sb + img;
   size_t chunk = std::max<size_t>(1, budget / per);
   chunk = std::min(chunk, batch);
   h->last_ckpt = use_ckpt ? 1 : 0;
@@ -704,6 +855,25 @@ int mlb_hea_evaluate(mlb_hea_t* h, size_t batch, const double* params, double* e
     if (on_device) cudaMemcpy(grads, hG.data(), batch * P * sizeof(double), cudaMemcpyHostToDevice);
     else std::memcpy(grads, hG.data(), batch * P * sizeof(double));
   }
+  return MLB_OK;
+}
+
+int mlb_hea_set_fused_forward(mlb_hea_t* h, int mode) {
+  if (!h) return hfail(MLB_ERR_INVALID_ARG, "null problem");
+  if (mode < -1 || mode > 1) return hfail(MLB_ERR_INVALID_ARG, "mode must be -1, 0 or 1");
+  if (mode == 1 && !h->fused_ok)
+    return hfail(MLB_ERR_NOT_SUPPORTED, "no fused forward plan (complex64 and N >= 13 only)");
+  h->fused_mode = mode;
+  return MLB_OK;
+}
+
+int mlb_hea_last_forward_fused(const mlb_hea_t* h, int* fused, uint32_t* passes, uint32_t* blocks) {
+  if (!h) return hfail(MLB_ERR_INVALID_ARG, "null problem");
+  if (fused) *fused = h->last_fused;
+  size_t np = 0;
+  for (const auto& seg : h->fseg) np += seg.size();
+  if (passes) *passes = (uint32_t)np;
+  if (blocks) *blocks = (uint32_t)h->fblocks.size();
   return MLB_OK;
 }
 

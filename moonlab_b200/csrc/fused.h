@@ -269,6 +269,8 @@ inline int emit(const std::vector<mlb_op_t>& ops, uint32_t n, Plan& P,
         h++;
       }
     dp.num_tiles = 1ull << (n - kTileBits);
+    dp.vec_shift = 63;
+    dp.vec_images = 0;
     dp.block_begin = (uint32_t)P.dev_blocks.size();
     dp.num_blocks = (uint32_t)pp.blocks.size();
     for (int bi : pp.blocks) {

@@ -462,4 +462,58 @@ int launch_adj_reduce(const double* d_partials, uint64_t tiles_per_state, int nu
   return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
 }
 
+// ---------------------------------------------------------------------------
+// Per-vector squared norms of a batch of complex64 states and the division
+// of energies and gradients by them (the tensor-core forward sweep's norm
+// drift cancels: E and dE/dtheta both carry |psi|^2).  One CTA per vector,
+// a fixed-order tree: the result does not depend on scheduling.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void __launch_bounds__(256) k_batch_norm(const float2* __restrict__ psi, uint64_t dim,
+                                                    double* __restrict__ out) {
+  __shared__ double red[256];
+  const float2* v = psi + (uint64_t)blockIdx.x * dim;
+  double acc = 0.0;
+  for (uint64_t i = threadIdx.x; i < dim; i += 256) {
+    const float2 a = v[i];
+    acc += (double)a.x * a.x + (double)a.y * a.y;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
+// out = [B] energies, then [B][P] gradients
+__global__ void k_divide_by_norm(double* __restrict__ out, uint64_t batch, int num_params,
+                                 const double* __restrict__ nrm) {
+  const uint64_t total = batch * (uint64_t)(1 + num_params);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t b = i < batch ? i : (i - batch) / (uint64_t)num_params;
+    out[i] /= nrm[b];
+  }
+}
+}  // namespace
+
+int launch_batch_norm(const void* psi_c64, uint64_t dim, uint64_t batch, double* d_norm, cudaStream_t stream) {
+  if (batch == 0 || batch > 65535) return MLB_ERR_INVALID_ARG;
+  k_batch_norm<<<(unsigned)batch, 256, 0, stream>>>(static_cast<const float2*>(psi_c64), dim, d_norm);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
+}
+
+int launch_divide_by_norm(double* d_out, uint64_t batch, int num_params, const double* d_norm,
+                          cudaStream_t stream) {
+  const uint64_t total = batch * (uint64_t)(1 + num_params);
+  uint64_t grid = (total + 255) / 256;
+  if (grid < 1) grid = 1;
+  if (grid > 148ull * 8) grid = 148ull * 8;
+  k_divide_by_norm<<<(unsigned)grid, 256, 0, stream>>>(d_out, batch, num_params, d_norm);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
+}
+
 }  // namespace mlb

@@ -319,15 +319,21 @@ __global__ void __launch_bounds__(kFThreads, 2)
   // as soon as application s's MMAs have completed.
   uint32_t ph_mma = 0, s = 0;
   bool bad = false;
+  // operand image of block b for tile t (per-vector image sets: the tile's
+  // vector picks its set)
+  auto image_of = [&](uint64_t t, uint32_t b) -> const uint8_t* {
+    return images + ((size_t)imgtab[b] + (size_t)(t >> pass.vec_shift) * pass.vec_images) * 16384;
+  };
   if (tid == 0) {
     const uint32_t nb = pass.num_blocks;
     if ((uint64_t)blockIdx.x < pass.num_tiles && !(test_skip_copy && blockIdx.x == 0)) {
       issued[0] = 1;
-      bulk_load(sbase + kBHi, images + (size_t)imgtab[0] * 16384, 16384, bar_b);
+      bulk_load(sbase + kBHi, image_of(blockIdx.x, 0), 16384, bar_b);
     }
-    if ((uint64_t)blockIdx.x + (nb > 1 ? 0ull : (uint64_t)gridDim.x) < pass.num_tiles) {
+    const uint64_t t1 = (uint64_t)blockIdx.x + (nb > 1 ? 0ull : (uint64_t)gridDim.x);
+    if (t1 < pass.num_tiles) {
       issued[1] = 1;
-      bulk_load(sbase + kBImg, images + (size_t)imgtab[nb > 1 ? 1 : 0] * 16384, 16384, bar_b + 8);
+      bulk_load(sbase + kBImg, image_of(t1, nb > 1 ? 1 : 0), 16384, bar_b + 8);
     }
   }
   float2* tile = reinterpret_cast<float2*>(sm + kTile0);
@@ -438,10 +444,10 @@ __global__ void __launch_bounds__(kFThreads, 2)
           if (!ok) atomicOr((int*)flag, 2);
           if (ok && warp == 5) {  // buffer s & 1 is free: application s + 2's image into it
             const uint32_t r = b + 2u, adv = r / pass.num_blocks, buf = s & 1u;
-            if (t + (uint64_t)adv * gridDim.x < pass.num_tiles) {
+            const uint64_t t2 = t + (uint64_t)adv * gridDim.x;
+            if (t2 < pass.num_tiles) {
               issued[buf] = issued[buf] + 1u;
-              bulk_load(sbase + buf * kBImg, images + (size_t)imgtab[r % pass.num_blocks] * 16384, 16384,
-                        bar_b + 8u * buf);
+              bulk_load(sbase + buf * kBImg, image_of(t2, r % pass.num_blocks), 16384, bar_b + 8u * buf);
             }
           }
         }
@@ -522,12 +528,78 @@ __global__ void __launch_bounds__(kFThreads, 2)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
 }
 
+// One operand image per (block, vector): thread c builds column c of the
+// block's 32x32 unitary in FP64 (the gates applied in order to basis vector
+// c, as the adjoint's forward passes apply them: RY = [[c, -s], [s, c]],
+// RZ = diag(c - i s, c + i s), X / CNOT a swap), then all threads write the
+// bf16 hi / lo split of U' in the swizzled K-major layout.
+__global__ void __launch_bounds__(128) k_fused_images(const FusedGenBlock* __restrict__ blocks, int num_blocks,
+                                                      const FusedGenOp* __restrict__ ops,
+                                                      const double2* __restrict__ cs, int num_params,
+                                                      uint8_t* __restrict__ images) {
+  __shared__ double2 U[32][33];  // U[row][column]
+  const int k = blockIdx.x, v = blockIdx.y, tid = threadIdx.x;
+  const FusedGenBlock blk = blocks[k];
+  if (tid < 32) {
+    const int c = tid;
+    for (int r = 0; r < 32; r++) U[r][c] = make_double2(r == c ? 1.0 : 0.0, 0.0);
+    for (uint32_t o = 0; o < blk.num_ops; o++) {
+      const FusedGenOp g = ops[blk.op_begin + o];
+      const uint32_t tb = 1u << g.lt;
+      const uint32_t cm = g.lc >= 0 ? (1u << g.lc) : 0u;
+      double2 t = make_double2(1.0, 0.0);
+      if (g.kind != ADJ_KIND_X) t = cs[(size_t)v * num_params + g.p];
+      for (uint32_t i = 0; i < 32; i++) {
+        if ((i & tb) || (i & cm) != cm) continue;
+        const double2 a0 = U[i][c], a1 = U[i | tb][c];
+        if (g.kind == ADJ_KIND_X) {
+          U[i][c] = a1;
+          U[i | tb][c] = a0;
+        } else if (g.kind == ADJ_KIND_RY) {
+          U[i][c] = make_double2(t.x * a0.x - t.y * a1.x, t.x * a0.y - t.y * a1.y);
+          U[i | tb][c] = make_double2(t.y * a0.x + t.x * a1.x, t.y * a0.y + t.x * a1.y);
+        } else {  // RZ: key 0 -> (c - i s), key 1 -> (c + i s)
+          U[i][c] = make_double2(t.x * a0.x + t.y * a0.y, t.x * a0.y - t.y * a0.x);
+          U[i | tb][c] = make_double2(t.x * a1.x - t.y * a1.y, t.x * a1.y + t.y * a1.x);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  uint16_t* hi = reinterpret_cast<uint16_t*>(images + ((size_t)v * num_blocks + k) * 16384);
+  uint16_t* lo = hi + 4096;
+  for (int idx = tid; idx < 64 * 64; idx += blockDim.x) {
+    const int rn = idx >> 6, kk = idx & 63;
+    const double2 u = U[rn & 31][kk & 31];
+    const double x = rn < 32 ? (kk < 32 ? u.x : -u.y) : (kk < 32 ? u.y : u.x);
+    const __nv_bfloat16 h = __float2bfloat16_rn((float)x);
+    const __nv_bfloat16 l = __float2bfloat16_rn((float)(x - (double)__bfloat162float(h)));
+    // element (rn, kk) at byte (rn / 8) * 1024 + (rn % 8) * 128 + 2 kk, 16-byte chunk xor rn % 8
+    const uint32_t off = (((uint32_t)(rn >> 3) * 1024u + (uint32_t)(rn & 7) * 128u + 2u * (uint32_t)kk) ^
+                          ((uint32_t)(rn & 7) << 4)) >> 1;
+    hi[off] = *reinterpret_cast<const uint16_t*>(&h);
+    lo[off] = *reinterpret_cast<const uint16_t*>(&l);
+  }
+}
+
 }  // namespace
+
+int launch_fused_images(const FusedGenBlock* blocks, int num_blocks, const FusedGenOp* ops, const double2* cs,
+                        int num_params, int batch, uint8_t* images, cudaStream_t stream) {
+  if (num_blocks < 1 || batch < 1 || batch > 65535 || !blocks || !ops || !cs || !images) return MLB_ERR_INVALID_ARG;
+  k_fused_images<<<dim3((unsigned)num_blocks, (unsigned)batch), 128, 0, stream>>>(blocks, num_blocks, ops, cs,
+                                                                                  num_params, images);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;
+}
 
 int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,
                       const uint8_t* d_images, int* d_err, int num_sms, cudaStream_t stream, int test_skip_copy) {
+  // n: bits of the tile enumeration (a batch of B states of N qubits: N +
+  // ceil(log2 B)); num_tiles may stop short of 2^(n - 13) (B not a power of 2)
   if (n < 13 || n > 13 + 4 * kTbNibbles || pass.num_blocks == 0 || pass.num_blocks > (uint32_t)kMaxBlocks ||
-      pass.num_low < 1 || pass.num_low + pass.num_high != 13 || pass.num_tiles != 1ull << (n - 13))
+      pass.num_low < 1 || pass.num_low + pass.num_high != 13 || pass.num_tiles == 0 ||
+      pass.num_tiles > 1ull << (n - 13) || pass.vec_shift > 63)
     return MLB_ERR_INVALID_ARG;
   static std::atomic<uint64_t> attr_set_mask{0};
   int dev = 0;

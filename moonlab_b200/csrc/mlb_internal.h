@@ -155,6 +155,11 @@ int launch_adj_pauli(int dtype, const void* psi, void* lam, const AdjPass& P, co
                      bool accumulate, bool energy, double* d_epart, int num_sms, cudaStream_t stream);
 int launch_adj_reduce(const double* d_partials, uint64_t tiles_per_state, int num_slots, uint64_t batch,
                       const int* d_param_of_slot, int num_params, double* d_out, cudaStream_t stream);
+// d_norm[b] = |psi_b|^2 of a complex64 batch; then d_out ([B] energies,
+// [B][P] gradients) divided by it.
+int launch_batch_norm(const void* psi_c64, uint64_t dim, uint64_t batch, double* d_norm, cudaStream_t stream);
+int launch_divide_by_norm(double* d_out, uint64_t batch, int num_params, const double* d_norm,
+                          cudaStream_t stream);
 
 // Gram matrix of B complex128 states stored back to back ([B][dim]):
 // d_G[a * B + b] = sum_x conj(S_a[x]) S_b[x] for a <= b (the rest of d_G is
@@ -234,6 +239,11 @@ struct FusedPassDev {
   uint64_t num_tiles;
   uint32_t block_begin;
   uint32_t num_blocks;
+  // per-vector operand images (a batch of states with their own matrices):
+  // tile t uses image (block image + (t >> vec_shift) * vec_images);
+  // vec_shift = 63 when every tile shares one set
+  uint32_t vec_shift;
+  uint32_t vec_images;
 };
 // ---- small circuits in one launch (kernels_small.cu; the serving path) ----
 // One request per item: ops[ops_off .. ops_off + num_ops) on an n-qubit
@@ -271,6 +281,26 @@ struct MailboxDev {
 };
 size_t mailbox_smem_bytes(int dtype);
 int launch_mailbox(int dtype, const MailboxDev& mb, int ctas, cudaStream_t stream);
+
+// ---- per-vector operand images of fused blocks (kernels_fused.cu) ----
+// A block's gates in the block's own 5 qubits (the local bit of a qubit is
+// the index of its tile position among the block's sorted positions), for
+// parameterised circuits whose angles differ per batch vector.
+struct FusedGenOp {
+  int8_t kind;  // ADJ_KIND_X (a CNOT when lc >= 0), ADJ_KIND_RY, ADJ_KIND_RZ
+  int8_t lt;    // local target bit
+  int8_t lc;    // local control bit, -1: none
+  int8_t pad;
+  int32_t p;    // parameter (RY, RZ): cs[vector * num_params + p] = (cos, sin) of half the angle
+};
+struct FusedGenBlock {
+  uint32_t op_begin, num_ops;
+};
+// images[(v * num_blocks + k) * 16 KiB]: block k's operand image for vector v,
+// the layout the fused host planner writes (bf16 hi and lo of
+// [Re U -Im U; Im U Re U], K-major, 128-byte swizzle).
+int launch_fused_images(const FusedGenBlock* blocks, int num_blocks, const FusedGenOp* ops, const double2* cs,
+                        int num_params, int batch, uint8_t* images, cudaStream_t stream);
 
 // d_err: device word set non-zero if a tensor-core completion wait ran out.
 int launch_fused_pass(void* amp, int n, const FusedPassDev& pass, const FusedBlockDev* d_blocks,

@@ -77,11 +77,22 @@ class HEAProblem:
         code = {"auto": 0, "always": 1, "never": -1}[mode]
         check(self._lib.mlb_hea_set_checkpointing(self._h, code), "mlb_hea_set_checkpointing")
 
+    def set_fused_forward(self, mode: str = "auto") -> None:
+        """complex64, N >= 13: the forward sweep on the tensor cores ('auto':
+        on when planned, 'on', 'off')."""
+        code = {"auto": 0, "on": 1, "off": -1}[mode]
+        check(self._lib.mlb_hea_set_fused_forward(self._h, code), "mlb_hea_set_fused_forward")
+
     def last_eval_stats(self) -> dict:
-        seg, used, chunks = C.c_uint32(), C.c_int(), C.c_size_t()
+        seg, used, chunks, fused = C.c_uint32(), C.c_int(), C.c_size_t(), C.c_int()
+        fp, fb = C.c_uint32(), C.c_uint32()
         check(self._lib.mlb_hea_last_eval_stats(self._h, C.byref(seg), C.byref(used), C.byref(chunks)),
               "mlb_hea_last_eval_stats")
-        return {"segment_layers": seg.value, "checkpoints": bool(used.value), "sub_batches": chunks.value}
+        check(self._lib.mlb_hea_last_forward_fused(self._h, C.byref(fused), C.byref(fp), C.byref(fb)),
+              "mlb_hea_last_forward_fused")
+        return {"segment_layers": seg.value, "checkpoints": bool(used.value), "sub_batches": chunks.value,
+                "fused_forward": bool(fused.value), "fused_forward_passes": fp.value,
+                "fused_forward_blocks": fb.value}
 
     def plan_stats(self):
         f, l, b = C.c_uint32(), C.c_uint32(), C.c_uint32()
