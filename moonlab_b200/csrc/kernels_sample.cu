@@ -17,11 +17,13 @@
 //    s, and only through the parity of s/g.  A chunk of elements therefore
 //    maps (N = s/g, parity) -> (N + K[parity], parity') with two integer
 //    increments, computed in parallel as an ordered reduction of 2-entry
-//    transfer tables (phase C).  Chunks are chained serially from the exact
-//    running value (phase D); a chunk whose sum leaves the binade, whose
-//    predicted binade was wrong, or which starts at s = 0 is summed element
-//    by element instead.  The binade of each chunk's start is predicted from
-//    an ordinary parallel prefix of chunk totals (phases A, B).
+//    transfer tables (phase C).  The tables compose associatively, so the
+//    chunks are chained from the exact running value by an ordered scan of
+//    their tables (phase D); a chunk whose sum leaves the binade, whose
+//    predicted binade was wrong, or which starts at s = 0 with a nonzero
+//    contribution is summed element by element instead.  The binade of each
+//    chunk's start is predicted from an ordinary parallel prefix of chunk
+//    totals (phases A, B).
 //  * Sampling (phase E): one warp per uniform finds the chunk whose exact
 //    end value first passes u and replays that chunk's adds in hardware
 //    FP64 (IEEE round to nearest, hence bit-identical).
@@ -46,6 +48,10 @@ constexpr int kCB = 12;             // chunk = 2^12 elements (33 KiB of p in sha
 constexpr int kCT = 256;            // threads per CTA
 constexpr int kPer = (1 << kCB) / kCT;  // 32 contiguous elements per thread
 constexpr long long kTwo53 = 1ll << 53;
+constexpr int kDPer = 16;               // phase D: chunks per thread in one scan
+constexpr int kDBatch = kCT * kDPer;     // phase D: 4096 chunks per scan
+constexpr int kNoBinade = -0x40000000;   // matches no candidate binade
+constexpr int kZeroChunk = 0x7fffffff;   // Xfer::e[0] of a chunk that adds 0 for every s
 
 struct Xfer {          // per chunk: transfer tables for two candidate binades
   int32_t e[2];        // binade exponents (INT32_MIN: unused)
@@ -236,7 +242,8 @@ __device__ __forceinline__ Fn elem_fn(double v, double inv_g) {
 template <typename Real, bool FUSED>
 __global__ void __launch_bounds__(kCT) k_seq_c(const typename Cplx<Real>::T* __restrict__ amp,
                                                uint64_t nc, uint32_t clen, uint64_t fmask,
-                                               uint64_t fval, const double* __restrict__ pre,
+                                               uint64_t fval, const double* __restrict__ ctot,
+                                               const double* __restrict__ pre,
                                                Xfer* __restrict__ xfer) {
   __shared__ double sp[(1 << kCB) + (1 << kCB) / 32];
   __shared__ Fn red[kCT / 32][2];
@@ -288,6 +295,10 @@ __global__ void __launch_bounds__(kCT) k_seq_c(const typename Cplx<Real>::T* __r
         x.K[cand][0] = a.K0; x.K[cand][1] = a.K1;
         x.P[cand][0] = a.P0; x.P[cand][1] = a.P1;
       }
+      // Every contribution is 0 exactly when the plain total is 0 (the
+      // values are >= 0; for FUSED, h*h rounds to 0 only below half the
+      // smallest subnormal, which then also leaves any s unchanged).
+      if (ctot[c] == 0.0) x.e[0] = kZeroChunk;
       xfer[c] = x;
     }
     (void)tot;
@@ -295,72 +306,121 @@ __global__ void __launch_bounds__(kCT) k_seq_c(const typename Cplx<Real>::T* __r
   }
 }
 
-// Phase D: serial chain over chunks (one CTA).  Transfer tables are staged
-// into shared memory in batches; thread 0 runs the integer fast path over a
-// batch; when a chunk cannot use it, all threads recompute that chunk's p
-// values into shared memory and thread 0 replays its adds.
-constexpr int kDBatch = 128;
+// Phase D: the exact running value at every chunk start, one CTA.  Transfer
+// tables compose associatively, so the chunks are taken kDBatch at a time
+// from the exact value b at the batch start: each thread composes the tables
+// of kDPer consecutive chunks for b's binade, the CTA scans those
+// compositions in order, and each thread walks its chunks again from its
+// exclusive prefix, writing s_in.  Increments are nonnegative, so the
+// running value only grows: the first chunk whose end leaves the binade, or
+// which has no table for it, is the first failure.  The values up to its
+// start are exact; that chunk is replayed element by element and the next
+// batch starts after it.  A chunk whose every contribution is 0 is the
+// identity for any s, so runs of such chunks pass even at s = 0.
+
+__device__ __forceinline__ Fn chunk_fn(const Xfer* __restrict__ xfer, uint64_t c, int e) {
+  const Xfer& x = xfer[c];
+  const int e0 = x.e[0], e1 = x.e[1];
+  if (e0 == kZeroChunk) return Fn{0, 0, 0, 1};
+  const int cand = (e0 == e) ? 0 : (e1 == e) ? 1 : -1;
+  if (cand < 0) return Fn{kTwo53, kTwo53, 0, 1};
+  return Fn{x.K[cand][0], x.K[cand][1], x.P[cand][0], x.P[cand][1]};
+}
+__device__ __forceinline__ Fn shfl_up_fn(const Fn& f, int o) {
+  Fn r;
+  r.K0 = __shfl_up_sync(0xffffffffu, f.K0, o);
+  r.K1 = __shfl_up_sync(0xffffffffu, f.K1, o);
+  r.P0 = __shfl_up_sync(0xffffffffu, f.P0, o);
+  r.P1 = __shfl_up_sync(0xffffffffu, f.P1, o);
+  return r;
+}
+
 template <typename Real, bool FUSED>
 __global__ void __launch_bounds__(kCT) k_seq_d(const typename Cplx<Real>::T* __restrict__ amp,
                                                uint64_t nc, uint32_t clen, uint64_t fmask,
                                                uint64_t fval, const Xfer* __restrict__ xfer,
                                                double* __restrict__ s_in) {
   __shared__ double sp[(1 << kCB) + (1 << kCB) / 32];
-  __shared__ Xfer sx[kDBatch];
-  __shared__ uint64_t s_next;
+  __shared__ Fn wtot[kCT / 32];
+  __shared__ unsigned int s_fail;
   __shared__ double s_run;
+  const Fn ident = {0, 0, 0, 1};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long* s_bits = (unsigned long long*)s_in;
   uint64_t c = 0;
-  double s = 0.0;
+  unsigned long long b = 0;  // bit pattern of the exact running value (s >= 0)
   while (c < nc) {
-    const uint64_t c0 = c, c1 = min(nc, c0 + kDBatch);
-    for (uint64_t i = c0 + threadIdx.x; i < c1; i += kCT) sx[i - c0] = xfer[i];
+    // s = N g in its binade; (N + K) g has the bit pattern b + K while
+    // N + K < 2^53, i.e. while b + K stays below `limit` (for a subnormal s
+    // the grid 2^-1074 also covers the lowest normal binade).
+    const int ex = (int)(b >> 52);
+    int e;
+    unsigned long long limit;
+    if (b == 0ull) { e = kNoBinade; limit = 1; }                // only all-zero chunks pass
+    else if (ex == 0x7ff) { e = kNoBinade; limit = 0; }         // inf / nan: replayed
+    else {
+      e = ex ? ex - 1023 : -1023;
+      limit = ex ? ((unsigned long long)(ex + 1) << 52) : (2ull << 52);
+    }
+    const int pb = (int)(b & 1ull);
+    const uint64_t c0 = c;
+    const uint64_t lo = c0 + (uint64_t)threadIdx.x * kDPer;
+    Fn acc = ident;
+#pragma unroll 4
+    for (int k = 0; k < kDPer; k++)
+      if (lo + k < nc) acc = compose(acc, chunk_fn(xfer, lo + k, e));
+    for (int o = 1; o < 32; o <<= 1) {  // inclusive scan over the warp, in order
+      const Fn other = shfl_up_fn(acc, o);
+      if (lane >= o) acc = compose(other, acc);
+    }
+    if (lane == 31) wtot[warp] = acc;
+    if (threadIdx.x == 0) s_fail = 0xffffffffu;
     __syncthreads();
-    while (true) {
-      if (threadIdx.x == 0) {
-        // s in binade e is N g with g = 2^(e-52) the binade's grid: N is s's
-        // significand (its mantissa bits with the implicit bit; the raw bits
-        // for a subnormal), and (N + K) g, for N + K < 2^53, has the bit
-        // pattern bits(s) + K (subnormal and normal patterns are contiguous).
-        // So the chain runs on the bit pattern, with no division.
-        unsigned long long b = (unsigned long long)__double_as_longlong(s);
-        for (; c < c1; c++) {
-          s_in[c] = __longlong_as_double((long long)b);
-          const Xfer& x = sx[c - c0];
-          const int xe0 = x.e[0], xe1 = x.e[1];  // independent of s: loaded ahead
-          const long long k00 = x.K[0][0], k01 = x.K[0][1], k10 = x.K[1][0], k11 = x.K[1][1];
-          const int ex = (int)(b >> 52);  // s >= 0: no sign bit
-          if (b == 0ull || ex == 0x7ff) break;  // zero (or inf / nan): replayed
-          const int e = ex ? ex - 1023 : -1023;
-          const int cand = (xe0 == e) ? 0 : (xe1 == e) ? 1 : -1;
-          if (cand < 0) break;
-          const long long N = ex ? (long long)((b & 0xfffffffffffffull) | 0x10000000000000ull) : (long long)b;
-          const long long K = cand == 0 ? ((b & 1ull) ? k01 : k00) : ((b & 1ull) ? k11 : k10);
-          if (N + K >= kTwo53) break;
-          b += (unsigned long long)K;
-        }
-        s = __longlong_as_double((long long)b);
-        s_next = c;
-        s_run = s;
+    Fn pre = ident;
+    for (int w = 0; w < warp; w++) pre = compose(pre, wtot[w]);
+    const Fn lane_ex = shfl_up_fn(acc, 1);
+    if (lane > 0) pre = compose(pre, lane_ex);
+    // walk this thread's chunks from the exact entry state (increment, parity)
+    long long kin = pb ? pre.K1 : pre.K0;
+    int par = pb ? pre.P1 : pre.P0;
+#pragma unroll 4
+    for (int k = 0; k < kDPer; k++) {
+      const uint64_t i = lo + k;
+      if (i >= nc) break;
+      s_bits[i] = b + (unsigned long long)kin;
+      const Fn f = chunk_fn(xfer, i, e);
+      kin = sat_add(kin, par ? f.K1 : f.K0);
+      par = par ? f.P1 : f.P0;
+      if (b + (unsigned long long)kin >= limit) {
+        atomicMin(&s_fail, (unsigned int)(i - c0));
+        break;
       }
-      __syncthreads();
-      c = s_next;
-      s = s_run;
-      if (c >= c1) break;
-      // element-by-element replay of chunk c
-      load_chunk_p<Real, FUSED>(amp, c * clen, clen, fmask, fval, sp);
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        for (uint32_t j = 0; j < clen; j++) s = elem_add<FUSED>(s, sp[j + (j >> 5)]);
-        s_run = s;
-      }
-      __syncthreads();
-      s = s_run;
-      c++;
-      __syncthreads();
     }
     __syncthreads();
+    const unsigned int fail = s_fail;
+    if (fail == 0xffffffffu) {
+      Fn tot = ident;
+      for (int w = 0; w < kCT / 32; w++) tot = compose(tot, wtot[w]);
+      b += (unsigned long long)(pb ? tot.K1 : tot.K0);
+      c = min(nc, c0 + (uint64_t)kDBatch);
+      __syncthreads();  // wtot is rewritten by the next batch
+      continue;
+    }
+    // element-by-element replay of the first failing chunk from its exact start
+    c = c0 + fail;
+    load_chunk_p<Real, FUSED>(amp, c * clen, clen, fmask, fval, sp);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = __longlong_as_double((long long)s_bits[c]);
+      for (uint32_t j = 0; j < clen; j++) s = elem_add<FUSED>(s, sp[j + (j >> 5)]);
+      s_run = s;
+    }
+    __syncthreads();
+    b = (unsigned long long)__double_as_longlong(s_run);
+    c++;
+    __syncthreads();
   }
-  if (threadIdx.x == 0) s_in[nc] = s;
+  if (threadIdx.x == 0) s_bits[nc] = b;
 }
 
 // Phase E: one warp per uniform.
@@ -467,7 +527,8 @@ int seq_prepare(const void* amp_v, int n, uint64_t fmask, uint64_t fval, size_t 
   const int grid = (int)std::min<uint64_t>(nc, (uint64_t)num_sms * 4);
   k_seq_a<Real, FUSED><<<grid, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.chunk_tot, sc.lastnz);
   k_seq_b<<<1, 1024, 0, stream>>>(sc.chunk_tot, nc, sc.chunk_pre);
-  k_seq_c<Real, FUSED><<<grid, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.chunk_pre, sc.xfer);
+  k_seq_c<Real, FUSED><<<grid, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.chunk_tot,
+                                                 sc.chunk_pre, sc.xfer);
   k_seq_d<Real, FUSED><<<1, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.xfer, sc.s_in);
   count_launch(4);
   return cudaGetLastError() == cudaSuccess ? MLB_OK : MLB_ERR_DRIVER;

@@ -309,6 +309,53 @@ def test_sampling_bit_exact_adversarial(gpu, n):
         assert np.array_equal(gt, B.port_measure_all_indices(a, u)), name
 
 
+def _large_states(n):
+    """States for the chunk-scan path at 2^(n-12) chunks (several 4096-chunk
+    scans): leading runs of all-zero chunks longer than a scan, probabilities
+    spread over ~1000 binades, and a dense random state.  Made one at a time."""
+    d = 1 << n
+    rng = np.random.default_rng(1000 + n)
+    basis = np.zeros(d, complex)
+    basis[d - d // 3] = 1
+    yield "basis", basis
+    del basis
+    half = np.zeros(d, complex)
+    half[d // 2:] = rng.standard_normal(d // 2) + 1j * rng.standard_normal(d // 2)
+    half /= np.linalg.norm(half)
+    yield "zero_then_random", half
+    del half
+    rnd = rng.standard_normal(d) + 1j * rng.standard_normal(d)
+    rnd /= np.linalg.norm(rnd)
+    yield "random", rnd
+    rnd *= np.exp(-rng.uniform(0, 300, d))
+    rnd[d // 5] = 1.0
+    rnd /= np.linalg.norm(rnd)
+    yield "tiny", rnd
+
+
+def test_sampling_bit_exact_many_scan_batches(gpu):
+    n = 26
+    rng = np.random.default_rng(26)
+    for name, a in _large_states(n):
+        cdf = cdf_of(a)
+        picks = cdf[rng.integers(0, a.size, 100)]
+        u = np.concatenate([picks, np.nextafter(picks, 0), np.nextafter(picks, 1), rng.random(200)])
+        u = u[(u >= 0) & (u < 1)]
+        del cdf
+        with StateVector(n) as sv:
+            sv.set_amplitudes(a)
+            ge = sv.sample(u, _lib.MLB_SAMPLE_CDF_GE)
+            u_gt = u[::40]  # the oracle walks the whole state once per uniform here
+            gt = sv.sample(u_gt, _lib.MLB_SAMPLE_CUM_GT)
+            av = np.ascontiguousarray(a).view(np.float64)
+            for q in (0, n - 1):
+                p = C.c_double()
+                _lib.check(_lib.load().mlb_prob_one_exact(sv.handle, q, C.byref(p)), "prob_one_exact")
+                assert p.value == B.port().svo_probability_one(_dp(av), n, q), (name, q)
+        assert np.array_equal(ge, B.port_sample(a, u)), name
+        assert np.array_equal(gt, B.port_measure_all_indices(a, u_gt)), name
+
+
 @pytest.mark.parametrize("n", [6, 14, 21])
 def test_exact_sequential_sums(gpu, n):
     for name, a in _states(n).items():
