@@ -48,15 +48,16 @@ constexpr int kCB = 12;             // chunk = 2^12 elements (33 KiB of p in sha
 constexpr int kCT = 256;            // threads per CTA
 constexpr int kPer = (1 << kCB) / kCT;  // 32 contiguous elements per thread
 constexpr long long kTwo53 = 1ll << 53;
-constexpr int kDPer = 16;               // phase D: chunks per thread in one scan
-constexpr int kDBatch = kCT * kDPer;     // phase D: 4096 chunks per scan
+constexpr int kDPer = 8;                // phase D: chunks per thread in one scan
+constexpr int kDBatch = kCT * kDPer;     // phase D: 2048 chunks per scan
 constexpr int kNoBinade = -0x40000000;   // matches no candidate binade
 constexpr int kZeroChunk = 0x7fffffff;   // Xfer::e[0] of a chunk that adds 0 for every s
 
-struct Xfer {          // per chunk: transfer tables for two candidate binades
-  int32_t e[2];        // binade exponents (INT32_MIN: unused)
+struct alignas(16) Xfer {  // per chunk: transfer tables for two candidate binades (3 x 16 bytes)
+  int32_t e[2];        // binade exponents (INT32_MIN: unused; e[0] == kZeroChunk: adds 0 for every s)
+  int32_t P;           // exit parities: bit 2 cand + entry parity
+  int32_t pad;
   long long K[2][2];   // [candidate][entry parity] increments, saturated at 2^53
-  int32_t P[2][2];     // exit parity
 };
 
 struct SeqScratch {
@@ -94,10 +95,6 @@ template <bool FUSED>
 __device__ __forceinline__ double elem_add(double s, double v) {
   return FUSED ? __fma_rn(v, v, s) : __dadd_rn(s, v);
 }
-template <bool FUSED>
-__device__ __forceinline__ double elem_approx(double v) {
-  return FUSED ? v * v : v;
-}
 
 // binade exponent of s > 0 (s in [2^e, 2^(e+1))) and its grid spacing
 __device__ __forceinline__ int binade_of(double s) {
@@ -122,44 +119,78 @@ __device__ __forceinline__ void load_chunk_p(const typename Cplx<Real>::T* __res
     sp[j + (j >> 5)] = elem_val<Real, FUSED>(amp, base + j, fmask, fval);
 }
 
-// Phase A: chunk totals (plain FP64, ordered) and the last nonzero index.
+// Phase A's per-element value: |a|^2 as x^2 + y^2, which is within a few
+// ulp of the reference's fl(cabs(a)^2).  The totals only predict each
+// chunk's binade (phase C allows ~10^6 ulp for it, and a wrong prediction
+// only sends the chunk to the exact replay), so glibc's algorithm is needed
+// only where the approximation could disagree on p > 0 (the last nonzero
+// index must be exact): below 2^-1000, and for inf / nan.
+template <typename Real, bool FUSED>
+__device__ __forceinline__ double elem_p_approx(const typename Cplx<Real>::T* __restrict__ amp, uint64_t i,
+                                                uint64_t fmask, uint64_t fval) {
+  if ((i & fmask) != fval) return 0.0;
+  const auto a = amp[i];
+  const double x = (double)a.x, y = (double)a.y;
+  const double pa = fma(x, x, y * y);
+  if (pa >= 0x1p-1000 && pa <= 0x1.fffffffffffffp+1023) return pa;
+  const double h = glibc_cabs(x, y);
+  return FUSED ? h * h : __dmul_rn(h, h);
+}
+
+// Phase C's per-element value for SEPARATE, on the candidate grids of the
+// chunk (inv_g = 1/g; 0: no such candidate).  Element transfer (elem_fn)
+// uses only k = p/g rounded to nearest.  x^2 + y^2 (one fma) is within
+// 2^-50 p of the reference's fl(cabs(a)^2): hypot is within one ulp and each
+// side rounds once more (2^-51 measured against glibc on 2*10^8 inputs).  So
+// where x^2 + y^2, scaled to a grid, lies more than 2^-48 of itself away from
+// a half-integer (and below 2^52), both round to the same k, no tie occurs,
+// and elem_fn gives the same transfer; elsewhere glibc's algorithm is used.
+__device__ __forceinline__ bool grid_safe(double pa, double inv_g) {
+  const double q = pa * inv_g;  // exact scaling by a power of two
+  if (!(q < 0x1p52)) return false;
+  const double fr = q - floor(q);
+  return fabs(fr - 0.5) > q * 0x1p-48;
+}
+template <typename Real>
+__device__ __forceinline__ double elem_p_on_grids(const typename Cplx<Real>::T* __restrict__ amp, uint64_t i,
+                                                  uint64_t fmask, uint64_t fval, double ig0, double ig1) {
+  if ((i & fmask) != fval) return 0.0;
+  const auto a = amp[i];
+  const double x = (double)a.x, y = (double)a.y;
+  const double pa = fma(x, x, y * y);
+  if (pa >= 0x1p-1000 && grid_safe(pa, ig0) && grid_safe(pa, ig1)) return pa;
+  return glibc_prob(x, y);
+}
+
+// Phase A: chunk totals (plain FP64, in a fixed order) and the last nonzero
+// index.  One warp per chunk, lane-strided coalesced loads; the order of the
+// additions does not matter here, so there is no staging and no barrier.
 template <typename Real, bool FUSED>
 __global__ void __launch_bounds__(kCT) k_seq_a(const typename Cplx<Real>::T* __restrict__ amp,
                                                uint64_t nc, uint32_t clen, uint64_t fmask,
                                                uint64_t fval, double* __restrict__ chunk_tot,
                                                long long* __restrict__ lastnz) {
-  __shared__ double sp[(1 << kCB) + (1 << kCB) / 32];
-  __shared__ double red[kCT / 32];
-  __shared__ long long redl[kCT / 32];
-  for (uint64_t c = blockIdx.x; c < nc; c += gridDim.x) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = (uint64_t)gridDim.x * (kCT / 32);
+  long long lnz_all = -1;
+  for (uint64_t c = (uint64_t)blockIdx.x * (kCT / 32) + (threadIdx.x >> 5); c < nc; c += nwarps) {
     const uint64_t base = c * clen;
-    load_chunk_p<Real, FUSED>(amp, base, clen, fmask, fval, sp);
-    __syncthreads();
     double t = 0.0;
     long long lnz = -1;
-    for (int k = 0; k < kPer; k++) {
-      const uint32_t j = threadIdx.x * kPer + k;
-      if (j < clen) {
-        const double p = elem_approx<FUSED>(sp[j + (j >> 5)]);
-        t += p;
-        if (p > 0.0) lnz = (long long)(base + j);
-      }
+#pragma unroll 8
+    for (uint32_t j = lane; j < clen; j += 32) {
+      const double p = elem_p_approx<Real, FUSED>(amp, base + j, fmask, fval);
+      t += p;
+      if (p > 0.0) lnz = (long long)(base + j);
     }
     for (int o = 16; o > 0; o >>= 1) {
       t += __shfl_down_sync(0xffffffffu, t, o);
       lnz = max(lnz, __shfl_down_sync(0xffffffffu, lnz, o));
     }
-    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = t; redl[threadIdx.x >> 5] = lnz; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double tt = 0.0;
-      long long ll = -1;
-      for (int w = 0; w < kCT / 32; w++) { tt += red[w]; ll = max(ll, redl[w]); }
-      chunk_tot[c] = tt;
-      if (ll >= 0) atomicMax(lastnz, ll);
-    }
-    __syncthreads();
+    if (lane == 0) chunk_tot[c] = t;
+    lnz_all = max(lnz_all, lnz);
   }
+  if (lane == 0 && lnz_all >= 0) atomicMax(lastnz, lnz_all);
 }
 
 // Phase B: exclusive prefix of chunk totals (one CTA; fixed order).
@@ -261,17 +292,25 @@ __global__ void __launch_bounds__(kCT) k_seq_c(const typename Cplx<Real>::T* __r
       ecand[1] = (ehi == elo) ? INT32_MIN : ehi;
       if (ehi - elo > 1) { ecand[0] = INT32_MIN; ecand[1] = INT32_MIN; }  // too uncertain
     }
-    load_chunk_p<Real, FUSED>(amp, base, clen, fmask, fval, sp);
+    const double ig0 = ecand[0] != INT32_MIN ? 1.0 / grid_of(ecand[0]) : 0.0;  // exact: powers of two
+    const double ig1 = ecand[1] != INT32_MIN ? 1.0 / grid_of(ecand[1]) : 0.0;
+    if constexpr (FUSED) {
+      load_chunk_p<Real, true>(amp, base, clen, fmask, fval, sp);
+    } else {
+      for (uint32_t j = threadIdx.x; j < clen; j += kCT)
+        sp[j + (j >> 5)] = elem_p_on_grids<Real>(amp, base + j, fmask, fval, ig0, ig1);
+    }
     __syncthreads();
-    Fn tot[2];
     for (int cand = 0; cand < 2; cand++) {
       Fn acc = {0, 0, 0, 1};  // identity
-      if (ecand[cand] != INT32_MIN) {
-        const double inv_g = 1.0 / grid_of(ecand[cand]);
-        for (int k = 0; k < kPer; k++) {
-          const uint32_t j = threadIdx.x * kPer + k;
-          if (j < clen) acc = compose(acc, elem_fn<FUSED>(sp[j + (j >> 5)], inv_g));
-        }
+      if (ecand[cand] == INT32_MIN) {  // no such candidate (uniform over the CTA)
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][cand] = acc;
+        continue;
+      }
+      const double inv_g = cand ? ig1 : ig0;
+      for (int k = 0; k < kPer; k++) {
+        const uint32_t j = threadIdx.x * kPer + k;
+        if (j < clen) acc = compose(acc, elem_fn<FUSED>(sp[j + (j >> 5)], inv_g));
       }
       // ordered warp reduction: lane l combines [l, l+o) with [l+o, l+2o)
       for (int o = 1; o < 32; o <<= 1) {
@@ -283,25 +322,26 @@ __global__ void __launch_bounds__(kCT) k_seq_c(const typename Cplx<Real>::T* __r
         if ((threadIdx.x & 31) + o < 32 && ((threadIdx.x & (2 * o - 1)) == 0)) acc = compose(acc, other);
       }
       if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][cand] = acc;
-      tot[cand] = acc;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       Xfer x;
+      int pbits = 0;
       for (int cand = 0; cand < 2; cand++) {
         Fn a = {0, 0, 0, 1};
         for (int w = 0; w < kCT / 32; w++) a = compose(a, red[w][cand]);
         x.e[cand] = ecand[cand];
         x.K[cand][0] = a.K0; x.K[cand][1] = a.K1;
-        x.P[cand][0] = a.P0; x.P[cand][1] = a.P1;
+        pbits |= (a.P0 | (a.P1 << 1)) << (2 * cand);
       }
+      x.P = pbits;
+      x.pad = 0;
       // Every contribution is 0 exactly when the plain total is 0 (the
       // values are >= 0; for FUSED, h*h rounds to 0 only below half the
       // smallest subnormal, which then also leaves any s unchanged).
       if (ctot[c] == 0.0) x.e[0] = kZeroChunk;
       xfer[c] = x;
     }
-    (void)tot;
     __syncthreads();
   }
 }
@@ -318,13 +358,16 @@ __global__ void __launch_bounds__(kCT) k_seq_c(const typename Cplx<Real>::T* __r
 // batch starts after it.  A chunk whose every contribution is 0 is the
 // identity for any s, so runs of such chunks pass even at s = 0.
 
+// Chunk c's map for binade e: three independent 16-byte loads, then a select.
 __device__ __forceinline__ Fn chunk_fn(const Xfer* __restrict__ xfer, uint64_t c, int e) {
-  const Xfer& x = xfer[c];
-  const int e0 = x.e[0], e1 = x.e[1];
-  if (e0 == kZeroChunk) return Fn{0, 0, 0, 1};
-  const int cand = (e0 == e) ? 0 : (e1 == e) ? 1 : -1;
+  const int4 h = __ldg(reinterpret_cast<const int4*>(xfer + c));
+  const longlong2 k0 = __ldg(reinterpret_cast<const longlong2*>(xfer + c) + 1);
+  const longlong2 k1 = __ldg(reinterpret_cast<const longlong2*>(xfer + c) + 2);
+  if (h.x == kZeroChunk) return Fn{0, 0, 0, 1};
+  const int cand = (h.x == e) ? 0 : (h.y == e) ? 1 : -1;
   if (cand < 0) return Fn{kTwo53, kTwo53, 0, 1};
-  return Fn{x.K[cand][0], x.K[cand][1], x.P[cand][0], x.P[cand][1]};
+  const int pb = h.z >> (2 * cand);
+  return cand == 0 ? Fn{k0.x, k0.y, pb & 1, (pb >> 1) & 1} : Fn{k1.x, k1.y, pb & 1, (pb >> 1) & 1};
 }
 __device__ __forceinline__ Fn shfl_up_fn(const Fn& f, int o) {
   Fn r;
@@ -365,10 +408,13 @@ __global__ void __launch_bounds__(kCT) k_seq_d(const typename Cplx<Real>::T* __r
     const int pb = (int)(b & 1ull);
     const uint64_t c0 = c;
     const uint64_t lo = c0 + (uint64_t)threadIdx.x * kDPer;
+    // this thread's chunk maps, loaded together and kept for both walks
+    Fn f[kDPer];
+#pragma unroll
+    for (int k = 0; k < kDPer; k++) f[k] = lo + k < nc ? chunk_fn(xfer, lo + k, e) : ident;
     Fn acc = ident;
-#pragma unroll 4
-    for (int k = 0; k < kDPer; k++)
-      if (lo + k < nc) acc = compose(acc, chunk_fn(xfer, lo + k, e));
+#pragma unroll
+    for (int k = 0; k < kDPer; k++) acc = compose(acc, f[k]);
     for (int o = 1; o < 32; o <<= 1) {  // inclusive scan over the warp, in order
       const Fn other = shfl_up_fn(acc, o);
       if (lane >= o) acc = compose(other, acc);
@@ -383,17 +429,18 @@ __global__ void __launch_bounds__(kCT) k_seq_d(const typename Cplx<Real>::T* __r
     // walk this thread's chunks from the exact entry state (increment, parity)
     long long kin = pb ? pre.K1 : pre.K0;
     int par = pb ? pre.P1 : pre.P0;
-#pragma unroll 4
+    bool walking = true;
+#pragma unroll
     for (int k = 0; k < kDPer; k++) {
       const uint64_t i = lo + k;
-      if (i >= nc) break;
-      s_bits[i] = b + (unsigned long long)kin;
-      const Fn f = chunk_fn(xfer, i, e);
-      kin = sat_add(kin, par ? f.K1 : f.K0);
-      par = par ? f.P1 : f.P0;
-      if (b + (unsigned long long)kin >= limit) {
-        atomicMin(&s_fail, (unsigned int)(i - c0));
-        break;
+      if (walking && i < nc) {
+        s_bits[i] = b + (unsigned long long)kin;
+        kin = sat_add(kin, par ? f[k].K1 : f[k].K0);
+        par = par ? f[k].P1 : f[k].P0;
+        if (b + (unsigned long long)kin >= limit) {
+          atomicMin(&s_fail, (unsigned int)(i - c0));
+          walking = false;
+        }
       }
     }
     __syncthreads();
@@ -412,6 +459,7 @@ __global__ void __launch_bounds__(kCT) k_seq_d(const typename Cplx<Real>::T* __r
     __syncthreads();
     if (threadIdx.x == 0) {
       double s = __longlong_as_double((long long)s_bits[c]);
+#pragma unroll 8
       for (uint32_t j = 0; j < clen; j++) s = elem_add<FUSED>(s, sp[j + (j >> 5)]);
       s_run = s;
     }
@@ -524,8 +572,11 @@ int seq_prepare(const void* amp_v, int n, uint64_t fmask, uint64_t fval, size_t 
   if (!sc.chunk_tot) return MLB_ERR_OUT_OF_MEMORY;
   const long long neg1 = -1;
   cudaMemcpyAsync(sc.lastnz, &neg1, sizeof(neg1), cudaMemcpyHostToDevice, stream);
-  const int grid = (int)std::min<uint64_t>(nc, (uint64_t)num_sms * 4);
-  k_seq_a<Real, FUSED><<<grid, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.chunk_tot, sc.lastnz);
+  // phase A: one warp per chunk, 5 CTAs per SM (its 48 registers allow 5);
+  // phase C: one CTA per chunk, 6 CTAs per SM (its shared memory allows 6)
+  const int grid_a = (int)std::min<uint64_t>((nc + kCT / 32 - 1) / (kCT / 32), (uint64_t)num_sms * 5);
+  const int grid = (int)std::min<uint64_t>(nc, (uint64_t)num_sms * 6);
+  k_seq_a<Real, FUSED><<<grid_a, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.chunk_tot, sc.lastnz);
   k_seq_b<<<1, 1024, 0, stream>>>(sc.chunk_tot, nc, sc.chunk_pre);
   k_seq_c<Real, FUSED><<<grid, kCT, 0, stream>>>(amp, nc, clen, fmask, fval, sc.chunk_tot,
                                                  sc.chunk_pre, sc.xfer);

@@ -288,7 +288,15 @@ def _states(n):
     tiny = rnd * np.exp(-rng.uniform(0, 300, d))  # probabilities down to ~1e-260
     tiny[d // 2] = 1.0
     tiny /= np.linalg.norm(tiny)
-    return dict(zero=zero, basis=basis, uniform=uniform, random=rnd, sparse=sparse, tiny=tiny)
+    # exact ties: the running sum stays in [0.5, 1) (grid 2^-53) and every
+    # other element adds exactly half a grid step (|2^-27|^2 = 2^-54), so the
+    # sum's rounding depends on its parity; the rest fill the sum towards 1
+    ties = np.zeros(d, complex)
+    ties[0] = 0.5 + 0.5j
+    ties[1::2] = 2.0 ** -27
+    rest = rnd[2::2] / np.linalg.norm(rnd[2::2]) * np.sqrt(0.49)
+    ties[2::2] = rest
+    return dict(zero=zero, basis=basis, uniform=uniform, random=rnd, sparse=sparse, tiny=tiny, ties=ties)
 
 
 @pytest.mark.parametrize("n", [5, 13, 22])
