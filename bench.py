@@ -307,13 +307,13 @@ def run_b200(args, ws, rank, local):
     torch.cuda.synchronize()
     launches0 = kernel_launches()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    pass_ms = []
+    step_gbs = []  # HBM bytes the step's launches moved / the step's device time
     with ClockSampler(local) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
             step()
             st = sv.flush_stats()  # waits for this step's kernels (device events)
-            pass_ms.append(st["gpu_ms"] / max(1, st["passes"]))
+            step_gbs.append(st["bytes_moved"] / max(1e-9, st["gpu_ms"] / 1e3) / 1e9)
         ev1.record(stream)
         ev1.synchronize()
     torch.cuda.synchronize()
@@ -325,13 +325,16 @@ def run_b200(args, ws, rank, local):
     passes = int(st["passes"])
     dense_segments = int(st["dense_blocks"])
     per_pass_bytes = 2 * 16 * (1 << n)
-    avg_pass_s = statistics.median(pass_ms) / 1e3
+    # After the reset that starts every step, the first passes run only over
+    # the tiles that can be nonzero; the engine counts the bytes its launches
+    # moved, and the roofline is taken over those bytes.
+    moved = int(st["bytes_moved"])
     peak, peak_kind = measured_peaks()
-    achieved = per_pass_bytes / avg_pass_s / 1e9
+    achieved = statistics.median(step_gbs)
     # the dense segments' FP64 tensor-core work: a 16x16 complex matrix on
     # every 16 amplitudes as three real 16x16 products (Gauss) = 48 real
     # multiply-adds (96 flops) per amplitude
-    dense_flops = dense_segments * 96.0 * (1 << n)
+    dense_flops = 96.0 * int(st["dense_amps"])  # over the tiles the launches ran over
 
     # the same c128 path with dense segments off: every register segment runs
     # gate by gate on the CUDA cores (no gate matrices multiplied together
@@ -393,8 +396,7 @@ def run_b200(args, ws, rank, local):
             maxerr = max(maxerr, float((aa - bb).abs().max().item()))
         s64.close()
         secs = statistics.median(t64)
-        per_pass = secs / max(1, st64["passes"])
-        gbs = 2 * 8 * (1 << n) / per_pass / 1e9
+        gbs = st64["bytes_moved"] / secs / 1e9  # the bytes the launches moved (all-zero tiles skipped)
         return {"circuit_ms": secs * 1e3, "speedup_vs_c128": t_max / secs,
                 "speedup_vs_c128_gate_by_gate": gbg_s / secs,
                 "fidelity": float(ip.abs().item() ** 2) / nb, "norm": nb, "max_amp_err": maxerr,
@@ -438,7 +440,9 @@ def run_b200(args, ws, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(n),
                          "kernel": "k_tile<double>", "peak_source": peak_kind,
-                         "algorithmic_bytes_per_pass": per_pass_bytes},
+                         "algorithmic_bytes_per_pass": per_pass_bytes,
+                         "bytes_moved_per_circuit": moved,
+                         "all_zero_tile_bytes_skipped": passes * per_pass_bytes - moved},
             # what bounds the c128 pass now: the FP64 tensor pipe (mma.sync f64)
             # running the dense segments; peak measured live (fp64_tensor_peak)
             "fp64_tensor": {"dense_segments": dense_segments, "segments": int(st["segments"]),

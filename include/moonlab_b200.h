@@ -396,11 +396,14 @@ typedef struct {
     uint64_t ops;
     uint64_t dense_blocks;   /* fused complex64 blocks, or complex128 segments run as dense
                                 matrices on the FP64 tensor cores */
-    uint64_t bytes_moved;    /* algorithmic HBM bytes of the launched passes */
+    uint64_t bytes_moved;    /* HBM bytes of the tiles the launched passes ran over (2 x state
+                                bytes per pass, less the tiles skipped as all-zero) */
     uint64_t kernel_launches;
     uint64_t segments;       /* shared-memory register-group round trips over all passes */
     double   gpu_ms;         /* device time of the flush's kernels (timing enabled), else 0 */
     uint64_t plan_cache_hit; /* 1 when the plan came from the state's plan cache */
+    uint64_t dense_amps;     /* complex128: amplitudes times dense segments applied to them
+                                (FP64 tensor-core work = 96 flops each) */
 } mlb_flush_stats_t;
 int  mlb_last_flush_stats(mlb_state_t *s, mlb_flush_stats_t *out);
 /* Plan cache for repeated circuit shapes (tiled mode): up to `entries` plans

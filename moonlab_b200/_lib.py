@@ -40,7 +40,7 @@ class MlbGate(C.Structure):
 class MlbFlushStats(C.Structure):
     _fields_ = [("passes", C.c_uint64), ("ops", C.c_uint64), ("dense_blocks", C.c_uint64),
                 ("bytes_moved", C.c_uint64), ("kernel_launches", C.c_uint64), ("segments", C.c_uint64),
-                ("gpu_ms", C.c_double), ("plan_cache_hit", C.c_uint64)]
+                ("gpu_ms", C.c_double), ("plan_cache_hit", C.c_uint64), ("dense_amps", C.c_uint64)]
 
 
 class MlbJobDesc(C.Structure):

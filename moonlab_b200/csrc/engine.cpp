@@ -114,6 +114,15 @@ struct mlb_state {
   int* h_ferr = nullptr;
   bool ferr_pending = false;
   bool test_skip_copy = false;  // mlb_test_fused_skip_copy: the next fused flush only
+  // Qubits that may be 1 in the index of a nonzero amplitude: every
+  // amplitude whose index has a bit outside `support` is exactly 0.  A reset
+  // makes it 0.  A tile pass mixes amplitudes only within its tiles, so it
+  // runs over the tiles whose outside bits lie in `support` (the others are
+  // zero and stay zero) and then adds its tile's qubits.  A write the engine
+  // cannot follow makes it all ones; once the device pointer has been handed
+  // out (`exposed`), writes through it cannot be followed at all.
+  uint64_t support = 0;
+  bool exposed = false;
   // plan cache for repeated circuit shapes (tiled mode; 0 entries = off)
   struct PlanEntry {
     std::vector<uint64_t> shape;              // the fused ops' shape words
@@ -495,14 +504,29 @@ int flush_fused(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   cudaMemsetAsync(s->d_ferr, 0, sizeof(int), s->stream);
   const int skip = s->test_skip_copy ? 1 : 0;
   s->test_skip_copy = false;
-  for (const auto& dp : P.dev_passes) {
+  // all-zero tiles (see mlb_state::support): a pass runs over the tiles whose
+  // outside bits may be nonzero, then adds its tile's qubits
+  const uint64_t allq = s->n >= 64 ? ~0ull : ((1ull << s->n) - 1ull);
+  const bool sparse = !s->exposed && (s->support & allq) != allq;
+  uint64_t sup = s->support;
+  for (size_t pi = 0; pi < P.dev_passes.size(); pi++) {
+    FusedPassDev dp = P.dev_passes[pi];
+    uint64_t tile = (1ull << dp.num_low) - 1ull;
+    for (int h = 0; h < dp.num_high; h++) tile |= 1ull << dp.hbits[h];
+    if (sparse) {
+      const uint64_t fm = allq & ~tile & sup;
+      dp.free_mask = (1ull << 63) | fm;
+      dp.num_tiles = 1ull << popc(fm);
+    }
+    sup |= tile & allq;
     rc = launch_fused_pass(s->amp, (int)s->n, dp, d_blocks, d_images, s->d_ferr, s->num_sms, s->stream,
-                           &dp == &P.dev_passes[0] ? skip : 0);
-    if (rc) return fail(rc, "fused pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+                           pi == 0 ? skip : 0);
+    if (rc) { s->support = ~0ull; return fail(rc, "fused pass launch failed: %s", cudaGetErrorString(cudaGetLastError())); }
     st.passes++;
     st.kernel_launches++;
-    st.bytes_moved += 2 * 8 * (1ull << s->n);
+    st.bytes_moved += 2 * 8 * (dp.num_tiles << (dp.num_low + dp.num_high));
   }
+  s->support = sup;
   cudaMemcpyAsync(s->h_ferr, s->d_ferr, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
   s->ferr_pending = true;
   st.ops += ops.size();
@@ -616,17 +640,42 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   const DevSegment* d_segs = reinterpret_cast<const DevSegment*>((unsigned char*)s->d_plan + soff);
   const DenseSegDev* d_dsegs = reinterpret_cast<const DenseSegDev*>((unsigned char*)s->d_plan + doff);
   const double* d_frags = reinterpret_cast<const double*>((unsigned char*)s->d_plan + foff);
-  auto launch_passes = [&]() -> int {
+  // Tiles that may hold nonzero amplitudes (see mlb_state::support): while
+  // some qubit has not been touched since a reset, a pass runs only over the
+  // tiles whose outside bits are touched ones.  Such launches depend on the
+  // state's history, so they are never captured into a cached graph.
+  const uint64_t allq = s->n >= 64 ? ~0ull : ((1ull << s->n) - 1ull);
+  const bool sparse = !s->exposed && (s->support & allq) != allq;
+  // HBM bytes and dense-segment amplitude applications of the launches
+  uint64_t moved = 0, dense_amps = 0;
+  auto launch_passes = [&](bool restrict) -> int {
+    uint64_t sup = s->support;
+    moved = dense_amps = 0;
     for (const auto& pp : E->passes) {
       bool all_dense = pp.pass.num_segments > 0;
-      for (int k = 0; k < pp.pass.num_segments; k++) all_dense = all_dense && dev_segs[pp.seg_begin + k].mode == 2;
-      const int r = launch_tile_pass(s->dtype, s->amp, pp.pass, d_segs + pp.seg_begin, d_ops, d_dsegs, d_frags,
+      int ndense = 0;
+      for (int k = 0; k < pp.pass.num_segments; k++) {
+        all_dense = all_dense && dev_segs[pp.seg_begin + k].mode == 2;
+        ndense += dev_segs[pp.seg_begin + k].mode == 2;
+      }
+      DevPass pass = pp.pass;
+      if (restrict) {
+        pass.tile_free_mask &= sup;
+        pass.num_tiles = 1ull << popc(pass.tile_free_mask);
+        sup |= allq & ~pp.pass.tile_free_mask;  // this pass's tile qubits
+      }
+      const uint64_t amps = pass.num_tiles << (pass.L + pass.H);
+      moved += 2 * ab * amps;
+      dense_amps += (uint64_t)ndense * amps;
+      const int r = launch_tile_pass(s->dtype, s->amp, pass, d_segs + pp.seg_begin, d_ops, d_dsegs, d_frags,
                                      s->num_sms, s->stream, all_dense);
       if (r) return r;
     }
     return MLB_OK;
   };
-  if (s->plan_cache_cap && E != &local) {
+  if (sparse) {
+    if ((rc = launch_passes(true))) return fail(rc, "tile pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  } else if (s->plan_cache_cap && E != &local) {
     // replay the captured launches (capture once per plan buffer)
     if (E->exec && E->graph_dplan != s->d_plan) {
       cudaGraphExecDestroy(E->exec);
@@ -637,7 +686,7 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
       cudaGraph_t g = nullptr;
       bool ok = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
       if (ok) {
-        const int lr = launch_passes();
+        const int lr = launch_passes(false);
         ok = cudaStreamEndCapture(s->stream, &g) == cudaSuccess && lr == MLB_OK && g;
         if (ok) ok = cudaGraphInstantiate(&E->exec, g, 0) == cudaSuccess;
         if (g) cudaGraphDestroy(g);
@@ -651,15 +700,21 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
     if (E->exec) {
       if (cudaGraphLaunch(E->exec, s->stream) != cudaSuccess)
         return fail(MLB_ERR_DRIVER, "graph launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-    } else if ((rc = launch_passes())) {
+    } else if ((rc = launch_passes(false))) {
       return fail(rc, "tile pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
-  } else if ((rc = launch_passes())) {
+  } else if ((rc = launch_passes(false))) {
     return fail(rc, "tile pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  for (const auto& pp : E->passes) s->support |= allq & ~pp.pass.tile_free_mask;
+  if (!sparse) {  // every tile of every pass (a replayed graph runs no launch_passes)
+    moved = E->passes.size() * 2 * ab * dim;
+    dense_amps = dsegs.size() << s->n;
   }
   st.passes += E->passes.size();
   st.kernel_launches += E->passes.size();
-  st.bytes_moved += E->passes.size() * 2 * ab * dim;
+  st.bytes_moved += moved;
+  st.dense_amps += dense_amps;
   st.ops += ops.size();
   st.segments += E->segs.size();
   st.dense_blocks += dsegs.size();
@@ -677,7 +732,8 @@ int flush_impl(mlb_state* s) {
     if (s->timing) cudaEventRecord(s->t0, s->stream);
     for (const auto& o : s->queue) {
       int rc = launch_gate(s->dtype, s->amp, (int)s->n, o, s->stream);
-      if (rc) { s->queue.clear(); return fail(rc, "gate launch failed: %s", cudaGetErrorString(cudaGetLastError())); }
+      if (rc) { s->queue.clear(); s->support = ~0ull; return fail(rc, "gate launch failed: %s", cudaGetErrorString(cudaGetLastError())); }
+      s->support |= op_targets(o);  // a gate mixes amplitudes that differ in its targets only
       st.ops++;
       st.passes++;
       st.kernel_launches++;
@@ -829,6 +885,7 @@ int mlb_state_create(uint32_t n, int dtype, int device, mlb_state_t** out) {
     mlb_state_free(s);
     return fail(rc, "init kernel");
   }
+  s->support = 0;  // |0...0>
   *out = s;
   return MLB_OK;
 }
@@ -871,6 +928,8 @@ int mlb_state_device_ptr(mlb_state_t* s, void** out) {
   if (!s || !out) return fail(MLB_ERR_INVALID_ARG, "null argument");
   int rc = flush_impl(s);
   if (rc) return rc;
+  s->exposed = true;  // writes through the pointer cannot be followed
+  s->support = ~0ull;
   *out = s->amp;
   return MLB_OK;
 }
@@ -956,7 +1015,9 @@ int mlb_state_reset(mlb_state_t* s) {
   if (!s) return fail(MLB_ERR_INVALID_ARG, "null state");
   DeviceGuard dg(s->device);
   s->queue.clear();
-  return launch_init_zero(s->dtype, s->amp, (int)s->n, s->stream);
+  const int rc = launch_init_zero(s->dtype, s->amp, (int)s->n, s->stream);
+  s->support = rc ? ~0ull : 0;  // |0...0>
+  return rc;
 }
 int mlb_state_copy_to_host(mlb_state_t* s, void* host) {
   if (!s || !host) return fail(MLB_ERR_INVALID_ARG, "null argument");
@@ -971,6 +1032,7 @@ int mlb_state_copy_from_host(mlb_state_t* s, const void* host) {
   if (!s || !host) return fail(MLB_ERR_INVALID_ARG, "null argument");
   DeviceGuard dg(s->device);
   s->queue.clear();  // the upload overwrites whatever was pending
+  s->support = ~0ull;
   cudaError_t e = cudaMemcpyAsync(s->amp, host, s->bytes, cudaMemcpyHostToDevice, s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "copy from host");
   return sync_stream(s);
@@ -981,6 +1043,7 @@ int mlb_state_copy(mlb_state_t* dst, mlb_state_t* src) {
   int rc = flush_impl(src);
   if (rc) return rc;
   dst->queue.clear();
+  dst->support = src->exposed ? ~0ull : src->support;
   DeviceGuard dg(dst->device);
   rc = sync_stream(src);
   if (rc) return rc;
@@ -1310,6 +1373,7 @@ int mlb_measure_all(mlb_state_t* s, double u, uint64_t* outcome) {
   if (rc) return rc;
   DeviceGuard dg(s->device);
   // collapse to |outcome>: zero everything, then write 1 at the index
+  s->support = ~0ull;
   cudaError_t e = cudaMemsetAsync(s->amp, 0, s->bytes, s->stream);
   if (e != cudaSuccess) return cuda_fail(e, "collapse memset");
   if (s->dtype == MLB_C128) {
@@ -1320,7 +1384,9 @@ int mlb_measure_all(mlb_state_t* s, double u, uint64_t* outcome) {
     e = cudaMemcpyAsync((char*)s->amp + 8 * (*outcome), one, 8, cudaMemcpyHostToDevice, s->stream);
   }
   if (e != cudaSuccess) return cuda_fail(e, "collapse write");
-  return sync_stream(s);
+  rc = sync_stream(s);
+  if (!rc) s->support = *outcome;  // only amplitude `outcome` is nonzero
+  return rc;
 }
 
 int mlb_normalize(mlb_state_t* s, double* norm_out) {
@@ -1476,6 +1542,7 @@ int mlb_plan_ops(const mlb_op_t* ops, size_t num, uint32_t n, int dtype, int fus
   st.ops = fused.size();
   st.kernel_launches = pl.passes.size();
   st.bytes_moved = st.passes * 2ull * (dtype == MLB_C128 ? 16ull : 8ull) * (1ull << n);
+  st.dense_amps = st.dense_blocks << n;  // a dense state: every tile of every pass
   *out = st;
   return MLB_OK;
 }

@@ -283,10 +283,10 @@ __global__ void __launch_bounds__(kFThreads, 2)
   for (int i = 0; i < 12; i++)
     if (i < (int)pass.num_high) hmask |= 1ull << pass.hbits[i];
   uint64_t* tbtab = reinterpret_cast<uint64_t*>(sm + kTbTab);
-  if (tid < kTbNibbles * 16) {  // entry (k, v): bits of v at set bits 4k .. 4k+3 of ~hmask
+  if (tid < kTbNibbles * 16) {  // entry (k, v): bits of v at set bits 4k .. 4k+3 of the free bits
     const int k = tid >> 4;
     const uint32_t v = (uint32_t)tid & 15u;
-    uint64_t m = ~hmask, g = 0;
+    uint64_t m = (pass.free_mask >> 63) ? (pass.free_mask & ~(1ull << 63)) : ~hmask, g = 0;
     for (int j = 0; j < 4 * k && m; j++) m &= m - 1;
     for (int i = 0; i < 4 && m; i++) {
       if (v >> i & 1u) g |= m & (~m + 1);

@@ -137,29 +137,32 @@ __device__ __forceinline__ double elem_p_approx(const typename Cplx<Real>::T* __
   return FUSED ? h * h : __dmul_rn(h, h);
 }
 
-// Phase C's per-element value for SEPARATE, on the candidate grids of the
-// chunk (inv_g = 1/g; 0: no such candidate).  Element transfer (elem_fn)
-// uses only k = p/g rounded to nearest.  x^2 + y^2 (one fma) is within
-// 2^-50 p of the reference's fl(cabs(a)^2): hypot is within one ulp and each
-// side rounds once more (2^-51 measured against glibc on 2*10^8 inputs).  So
-// where x^2 + y^2, scaled to a grid, lies more than 2^-48 of itself away from
-// a half-integer (and below 2^52), both round to the same k, no tie occurs,
-// and elem_fn gives the same transfer; elsewhere glibc's algorithm is used.
+// Phase C's per-element value, on the candidate grids of the chunk
+// (inv_g = 1/g; 0: no such candidate).  Element transfer (elem_fn) uses only
+// k = (contribution)/g rounded to nearest.  x^2 + y^2 (one fma) is within
+// 2^-50 of the contribution -- SEPARATE's fl(cabs(a)^2) and FUSED's exact
+// cabs(a)^2 -- as hypot is within one ulp and each side rounds once more
+// (2^-51 measured against glibc on 2*10^8 inputs).  So where x^2 + y^2,
+// scaled to a grid, lies more than 2^-48 of itself away from a half-integer
+// (and below 2^52), both round to the same k, no tie occurs, and elem_fn
+// gives the same transfer; elsewhere glibc's algorithm is used.  The value
+// kept is p for SEPARATE; for FUSED it is h, or -(x^2 + y^2) on the fast path.
 __device__ __forceinline__ bool grid_safe(double pa, double inv_g) {
   const double q = pa * inv_g;  // exact scaling by a power of two
   if (!(q < 0x1p52)) return false;
   const double fr = q - floor(q);
   return fabs(fr - 0.5) > q * 0x1p-48;
 }
-template <typename Real>
+template <typename Real, bool FUSED>
 __device__ __forceinline__ double elem_p_on_grids(const typename Cplx<Real>::T* __restrict__ amp, uint64_t i,
                                                   uint64_t fmask, uint64_t fval, double ig0, double ig1) {
   if ((i & fmask) != fval) return 0.0;
   const auto a = amp[i];
   const double x = (double)a.x, y = (double)a.y;
   const double pa = fma(x, x, y * y);
-  if (pa >= 0x1p-1000 && grid_safe(pa, ig0) && grid_safe(pa, ig1)) return pa;
-  return glibc_prob(x, y);
+  if (pa >= 0x1p-1000 && grid_safe(pa, ig0) && grid_safe(pa, ig1)) return FUSED ? -pa : pa;
+  const double h = glibc_cabs(x, y);
+  return FUSED ? h : __dmul_rn(h, h);
 }
 
 // Phase A: chunk totals (plain FP64, in a fixed order) and the last nonzero
@@ -236,13 +239,17 @@ __device__ __forceinline__ Fn compose(const Fn& f, const Fn& g) {  // g after f
 // r = qh - fl (exact), the nearest integer to q is fl + 1 when r > 1/2 or
 // (r == 1/2 and ql > 0), fl when r < 1/2 or (r == 1/2 and ql < 0), and a tie
 // only when r == 1/2 and ql == 0: |ql| <= ulp(qh)/2 and r lies on qh's
-// grid, so ql can only decide the case r == 1/2.
+// grid, so ql can only decide the case r == 1/2.  FUSED with v < 0: -v is
+// the contribution itself, x^2 + y^2 at a position where it rounds to the
+// same increment as h*h (elem_p_on_grids), with lo = 0.
 template <bool FUSED>
 __device__ __forceinline__ Fn elem_fn(double v, double inv_g) {
   Fn f;
   if (v == 0.0) { f.K0 = 0; f.K1 = 0; f.P0 = 0; f.P1 = 1; return f; }
   double hi = v, lo = 0.0;
-  if (FUSED) {
+  if (FUSED && v < 0.0) {
+    hi = -v;
+  } else if (FUSED) {
     hi = __dmul_rn(v, v);
     lo = __fma_rn(v, v, -hi);
     if (hi == 0.0) { f.K0 = 0; f.K1 = 0; f.P0 = 0; f.P1 = 1; return f; }
@@ -294,12 +301,8 @@ __global__ void __launch_bounds__(kCT) k_seq_c(const typename Cplx<Real>::T* __r
     }
     const double ig0 = ecand[0] != INT32_MIN ? 1.0 / grid_of(ecand[0]) : 0.0;  // exact: powers of two
     const double ig1 = ecand[1] != INT32_MIN ? 1.0 / grid_of(ecand[1]) : 0.0;
-    if constexpr (FUSED) {
-      load_chunk_p<Real, true>(amp, base, clen, fmask, fval, sp);
-    } else {
-      for (uint32_t j = threadIdx.x; j < clen; j += kCT)
-        sp[j + (j >> 5)] = elem_p_on_grids<Real>(amp, base + j, fmask, fval, ig0, ig1);
-    }
+    for (uint32_t j = threadIdx.x; j < clen; j += kCT)
+      sp[j + (j >> 5)] = elem_p_on_grids<Real, FUSED>(amp, base + j, fmask, fval, ig0, ig1);
     __syncthreads();
     for (int cand = 0; cand < 2; cand++) {
       Fn acc = {0, 0, 0, 1};  // identity

@@ -244,6 +244,10 @@ struct FusedPassDev {
   // vec_shift = 63 when every tile shares one set
   uint32_t vec_shift;
   uint32_t vec_images;
+  // bit 63 set: the tile index is deposited into the other set bits of
+  // free_mask (the pass runs over only those tiles); else into every bit
+  // outside the tile
+  uint64_t free_mask;
 };
 // ---- small circuits in one launch (kernels_small.cu; the serving path) ----
 // One request per item: ops[ops_off .. ops_off + num_ops) on an n-qubit

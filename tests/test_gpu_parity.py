@@ -110,6 +110,66 @@ def test_brickwork_eager_equals_tiled(gpu):
 
 
 # ---------------------------------------------------------------------------
+# all-zero tiles: after a reset, passes run only over tiles that may be nonzero
+# ---------------------------------------------------------------------------
+def test_zero_tiles_skipped_after_reset(gpu):
+    n = 22
+    g1 = brickwork(n, 6, 11, zz_every=2)
+    g2 = brickwork(n, 5, 12, zz_every=3)
+    full = 2 * 16 * (1 << n)
+    with StateVector(n) as sv, StateVector(n) as other:
+        # from |0...0>: the first passes touch a few tiles only
+        sv.run(g1)
+        a1 = sv.amplitudes()
+        st = sv.flush_stats()
+        assert np.abs(a1 - B.port_run(n, g1)).max() < TOL
+        assert st["bytes_moved"] < st["passes"] * full
+        assert st["dense_amps"] < st["dense_blocks"] << n
+        # a second circuit on the now dense state: every tile
+        sv.run(g2)
+        a12 = sv.amplitudes()
+        st = sv.flush_stats()
+        assert np.abs(a12 - B.port_run_from(n, g2, a1)).max() < TOL
+        assert st["bytes_moved"] == st["passes"] * full
+        # collapse to a basis state, then more gates: only its index is nonzero
+        k = sv.measure_all(0.61)
+        basis = np.zeros(1 << n, complex)
+        basis[k] = 1
+        assert np.array_equal(sv.amplitudes(), basis)
+        sv.run(g1)
+        assert np.abs(sv.amplitudes() - B.port_run_from(n, g1, basis)).max() < TOL
+        assert sv.flush_stats()["bytes_moved"] < sv.flush_stats()["passes"] * full
+        # a copy of a fresh state keeps its zero tiles; uploaded amplitudes do not
+        sv.reset()
+        other.copy_from(sv)
+        other.run(g2)
+        assert np.abs(other.amplitudes() - B.port_run(n, g2)).max() < TOL
+        assert other.flush_stats()["bytes_moved"] < other.flush_stats()["passes"] * full
+        other.set_amplitudes(a1)
+        other.run(g2)
+        assert np.abs(other.amplitudes() - a12).max() < TOL
+        assert other.flush_stats()["bytes_moved"] == other.flush_stats()["passes"] * full
+        # after the device pointer is handed out, every pass runs over every tile
+        other.device_ptr()
+        other.reset()
+        other.run(g1)
+        assert np.abs(other.amplitudes() - a1).max() < TOL
+        assert other.flush_stats()["bytes_moved"] == other.flush_stats()["passes"] * full
+    # the fused complex64 path skips the same tiles
+    with StateVector(n, "c64") as f:
+        f.run(g1)
+        got = f.amplitudes().astype(np.complex128)  # flushes
+        st = f.flush_stats()
+        assert abs(np.vdot(a1, got)) ** 2 / np.vdot(got, got).real >= 1 - 1e-6
+        assert 0 < st["bytes_moved"] < st["passes"] * (full // 2)
+        f.run(g2)
+        got = f.amplitudes().astype(np.complex128)
+        st = f.flush_stats()
+        assert abs(np.vdot(a12, got)) ** 2 / np.vdot(got, got).real >= 1 - 1e-6
+        assert st["bytes_moved"] == st["passes"] * (full // 2)
+
+
+# ---------------------------------------------------------------------------
 # QAOA: CNOT . RZ . CNOT lifted to one parity-phase op per edge
 # ---------------------------------------------------------------------------
 @pytest.mark.parametrize("n,mode,dense", [(12, "tiled", True), (16, "tiled", True), (16, "tiled", False),
