@@ -98,7 +98,11 @@ void mlb_state_free(mlb_state_t *s);
 int  mlb_state_num_qubits(const mlb_state_t *s, uint32_t *out);
 int  mlb_state_dim(const mlb_state_t *s, uint64_t *out);
 int  mlb_state_dtype(const mlb_state_t *s, int *out);
-int  mlb_state_device_ptr(mlb_state_t *s, void **out);   /* flushes first */
+/* The state's device buffer (flushes first).  After a reset, tile passes run
+ * only over the tiles that can hold nonzero amplitudes; once this pointer has
+ * been handed out, writes through it cannot be followed, so every later pass
+ * of this state runs over every tile. */
+int  mlb_state_device_ptr(mlb_state_t *s, void **out);
 int  mlb_state_set_stream(mlb_state_t *s, void *cuda_stream); /* NULL = own stream */
 int  mlb_state_stream(const mlb_state_t *s, void **cuda_stream); /* the stream kernels run on */
 int  mlb_state_set_exec_mode(mlb_state_t *s, int mode);
