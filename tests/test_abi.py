@@ -110,6 +110,7 @@ def test_planner_groups_the_brickwork_workloads():
     st = plan(g2, 30)
     assert st.passes <= 80                         # vs 4470 sweeps gate by gate
     assert st.bytes_moved == st.passes * 2 * 16 * (1 << 30)
+    assert st.dense_amps == st.dense_blocks << 30  # planned for a dense state: every tile
     # c128: 12-bit tiles (2 contiguous low qubits), a pass's short trailing
     # segment deferred to the next pass: a few more passes, fewer dense segments
     assert st.passes <= 66 and st.segments <= 150
