@@ -130,3 +130,72 @@ def test_live_against_reference_library():
             assert np.array_equal(got_state, ref_post)
             L.quantum_state_free(C.byref(cl))
         r.close()
+
+
+def test_numpy_op_reference_matches_the_oracle():
+    """The numpy reference of the random-op GPU tests (tests/ops_np.py) gives
+    the oracle's results for every op kind the oracle has a kernel for: 1q and
+    2q matrices, multi-controlled X and Z, SWAP, Fredkin, ZZ and the
+    controlled rotations (its control masking is the same code for 1q, X and
+    SWAP)."""
+    from ops_np import np_apply, rand_unitary
+    n = 7
+    rng = np.random.default_rng(77)
+    lib = B.port()
+
+    def gate(a, t, q0, q1=-1, q2=-1, th=0.0):
+        g = B.SvoGate(t, q0, q1, q2, th, 0.0, 0.0)
+        assert lib.svo_apply_gate(_dp(a.view(np.float64)), n, C.byref(g)) == 0
+
+    def rot(axis, th):
+        c, s = np.cos(th / 2), np.sin(th / 2)
+        if axis == "x":
+            return np.array([[c, -1j * s], [-1j * s, c]])
+        if axis == "y":
+            return np.array([[c, -s], [s, c]], complex)
+        return np.diag([np.exp(-0.5j * th), np.exp(0.5j * th)])
+
+    codes = {"x": 24, "y": 25, "z": 26}  # SVO_CRX, SVO_CRY, SVO_CRZ
+    for trial in range(60):
+        a = rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)
+        a /= np.linalg.norm(a)
+        q = [int(v) for v in rng.permutation(n)]
+        t, t2 = q[0], q[1]
+        ctrls = q[2:2 + int(rng.integers(0, 3))]
+        cmask = sum(1 << c for c in ctrls)
+        got = np.ascontiguousarray(a.copy())
+        kind = trial % 7
+        if kind == 0:
+            m = rand_unitary(rng, 2)
+            want = np_apply(a, n, "1q", t, -1, 0, m.reshape(4))
+            mm = np.ascontiguousarray(m.reshape(4)).view(np.float64)
+            lib.svo_apply_1q_matrix(_dp(got.view(np.float64)), n, t, _dp(mm))
+        elif kind == 1:
+            axis = "xyz"[trial % 3]
+            th = float(rng.uniform(-3, 3))
+            want = np_apply(a, n, "1q", t, -1, 1 << q[2], rot(axis, th).reshape(4))
+            gate(got, codes[axis], q[2], t, th=th)
+        elif kind == 2:
+            want = np_apply(a, n, "x", t, -1, cmask, None)
+            lib.svo_apply_mcx(_dp(got.view(np.float64)), n, cmask, t)
+        elif kind == 3:
+            m = rand_unitary(rng, 4)
+            want = np_apply(a, n, "2q", t, t2, 0, m.reshape(16))
+            mm = np.ascontiguousarray(m.reshape(16)).view(np.float64)
+            lib.svo_apply_2q_matrix(_dp(got.view(np.float64)), n, t, t2, _dp(mm))
+        elif kind == 4:
+            if trial % 2:
+                want = np_apply(a, n, "swap", t, t2, 0, None)
+                gate(got, 13, t, t2)  # SVO_SWAP
+            else:
+                want = np_apply(a, n, "swap", t, t2, 1 << q[2], None)
+                gate(got, 29, q[2], t, t2)  # SVO_FREDKIN
+        elif kind == 5:
+            th = float(rng.uniform(0, 6.28))
+            want = np_apply(a, n, "zz", t, t2, 0, np.array([np.exp(-0.5j * th), np.exp(0.5j * th)]))
+            gate(got, 27, t, t2, th=th)  # SVO_ZZ
+        else:
+            mask = (1 << t) | cmask
+            want = np_apply(a, n, "phase", 0, -1, mask, np.array([-1.0]))
+            lib.svo_apply_mcz(_dp(got.view(np.float64)), n, mask)
+        assert np.abs(got - want).max() < 1e-13, (trial, kind)
