@@ -646,10 +646,13 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   // state's history, so they are never captured into a cached graph.
   const uint64_t allq = s->n >= 64 ? ~0ull : ((1ull << s->n) - 1ull);
   const bool sparse = !s->exposed && (s->support & allq) != allq;
+  // until every launch went out, nothing is assumed about the state's zeros
+  const uint64_t sup0 = s->support;
+  s->support = ~0ull;
   // HBM bytes and dense-segment amplitude applications of the launches
   uint64_t moved = 0, dense_amps = 0;
   auto launch_passes = [&](bool restrict) -> int {
-    uint64_t sup = s->support;
+    uint64_t sup = sup0;
     moved = dense_amps = 0;
     for (const auto& pp : E->passes) {
       bool all_dense = pp.pass.num_segments > 0;
@@ -706,6 +709,7 @@ int flush_tiled(mlb_state* s, const std::vector<mlb_op_t>& ops, mlb_flush_stats_
   } else if ((rc = launch_passes(false))) {
     return fail(rc, "tile pass launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
+  s->support = sup0;
   for (const auto& pp : E->passes) s->support |= allq & ~pp.pass.tile_free_mask;
   if (!sparse) {  // every tile of every pass (a replayed graph runs no launch_passes)
     moved = E->passes.size() * 2 * ab * dim;
