@@ -234,7 +234,7 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
   const uint32_t glb = sg->g_lo[g8], gld0 = sg->g_lo[2 * q], gld1 = sg->g_lo[2 * q + 1];
   const double* fseg = frags + sg->frag_off + lane;
   int cur = -1;
-  double ar[8], aj[8];  // fragment (i, s) at index 4 i + s
+  double ar[8], aj[8], arj[8];  // fragment (i, s) at index 4 i + s; arj = ar + aj
   // two column tiles per step: 12 independent accumulator chains per warp
   // cover the DMMA latency; they differ only in bit 0 of j, so they share
   // their conditioning values (the top nloc <= 5 of j's 6 bits)
@@ -253,6 +253,8 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
         ar[k] = __ldg(f + 32 * k);
         aj[k] = __ldg(f + 32 * (8 + k));
       }
+#pragma unroll
+      for (int k = 0; k < 8; k++) arj[k] = ar[k] + aj[k];  // R + J, once per variant
       cur = var;
     }
     double2 x0[4], x1[4];  // this step's B operands (two column tiles)
@@ -279,7 +281,7 @@ __device__ __forceinline__ void dense_segment(double2* __restrict__ sm, const De
         dmma_f64(t[1][0][i][0], t[1][0][i][1], ar[f], x1[sk].x);
         dmma_f64(t[0][1][i][0], t[0][1][i][1], aj[f], x0[sk].y);
         dmma_f64(t[1][1][i][0], t[1][1][i][1], aj[f], x1[sk].y);
-        const double af = ar[f] + aj[f];  // R + J (kept out of registers between steps)
+        const double af = arj[f];
         dmma_f64(t[0][2][i][0], t[0][2][i][1], af, s0);
         dmma_f64(t[1][2][i][0], t[1][2][i][1], af, s1);
       }
